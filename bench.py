@@ -1,0 +1,397 @@
+"""Benchmark of the SSIMULACRA2 hot path: 1080p frame pairs per second on B200.
+
+Workload (the configuration the headline metric is quoted on): batches of 64 frame pairs,
+1920x1080 Y'CbCr 4:2:0, 10-bit limited range, BT.709 matrix/transfer/primaries, seeded
+synthetic content (sinusoid sums + noise, distorted by 8x8 DCT quantisation with per-frame
+steps in [4, 48] and the 4:2:0 chroma round trip).  One step scores one batch.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm prints one JSON line with
+  value       device-resident throughput (inputs already in HBM, VshipExt_ComputeSSIMU2Device
+              on 64 pairs per call), CUDA events on the launching stream, max over ranks;
+  e2e         the same metric through Vship_ComputeSSIMU2 with pinned host buffers
+              (host->device copies and the score read-back inside the timed region);
+  roofline    achieved HBM bandwidth of the dominant kernel (algorithmic bytes per launch /
+              its average CUDA-event launch duration) against MEASURED_PEAKS.json;
+  cpu_baseline  the FP64 oracle on all host cores, on a bounded sample of the same workload.
+The reference arm runs the unmodified Vship library built from its own sources
+(oracle/_ref/libvship_ref.so) through its own C API, with pinned host buffers and the
+best of several handler/thread counts, on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, BATCH = 1920, 1080, 64
+WORKLOAD = "ssimu2_1080p_yuv420p10_bt709_batch64"
+METRIC = "1080p SSIMU2 frame-pairs/s"
+UNIT = "frame-pairs/s"
+
+# Algorithmic bytes per 1080p pair (see DESIGN.md "Roofline"): the front kernel reads the
+# raw 10-bit 4:2:0 planes of both frames and writes the XYB planes the maps read; the maps
+# kernel reads those planes once.
+RAW_BYTES_PER_IMAGE = 1920 * 1080 * 2 + 2 * 960 * 540 * 2
+XYB_FLOATS_PER_IMAGE = 1920 * 1080 + 2 * 960 * 540 + 2 * 480 * 270 + 3 * 240 * 135 + 3 * 120 * 68
+ALGO_BYTES = {
+    "ssimu2_front": 2 * (RAW_BYTES_PER_IMAGE + 4 * XYB_FLOATS_PER_IMAGE),
+    "ssimu2_maps": 2 * 4 * XYB_FLOATS_PER_IMAGE,
+    "ssimu2_final": 0,
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = open(os.devnull, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=self.out, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            text, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            text = ""
+        rows = [l.split(",") for l in text.strip().splitlines() if l.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_workload(seed):
+    from vship_b200 import synth
+    t = time.time()
+    pairs = synth.make_pairs(BATCH, W, H, fmt="yuv420p10", seed=seed, unique=8, steps=(4.0, 48.0))
+    log("generated %d pairs in %.1fs" % (len(pairs), time.time() - t))
+    return pairs
+
+
+def input_bytes(pairs):
+    return sum(p.nbytes for pr in pairs for p in pr[0] + pr[1])
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from vship_b200 import abi, api
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    cs = abi.yuv420_10bit_bt709(W, H)
+    pairs = make_workload(seed=1234 + rank)
+    ls = pairs[0][2]
+
+    # ---------------- device-resident throughput (value) ----------------
+    dev = []
+    for p1, p2, _ in pairs:
+        dev.append(([torch.from_numpy(p.view(np.uint8)).cuda() for p in p1],
+                    [torch.from_numpy(p.view(np.uint8)).cuda() for p in p2]))
+    ptr1 = [t.data_ptr() for d in dev for t in d[0]]
+    ptr2 = [t.data_ptr() for d in dev for t in d[1]]
+    scores = torch.zeros(BATCH, dtype=torch.float64, device="cuda")
+    h = api.SSIMU2(cs, gpu_id=local)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        h.compute_device(BATCH, ptr1, ptr2, ls, ls, scores.data_ptr(), 0, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+    ms_per_step = ms / args.steps
+    value = BATCH * world * args.steps / (ms / 1e3)
+    dev_scores = scores.cpu().numpy()
+
+    # ---------------- per-kernel timing for the roofline ----------------
+    h.kernel_timing(True)
+    h.kernel_times(reset=True)
+    for _ in range(max(3, args.steps // 2)):
+        step()
+    torch.cuda.synchronize()
+    ktimes = h.kernel_times(reset=True)
+    h.kernel_timing(False)
+    top = max(ktimes.items(), key=lambda kv: kv[1][1])
+    top_name, (launches, total_ms) = top
+    avg_ms = total_ms / launches
+    peak, peak_kind = measured_peaks()
+    achieved = ALGO_BYTES[top_name] * BATCH / (avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": None, "algorithmic_bytes_per_launch": ALGO_BYTES[top_name] * BATCH,
+                "avg_launch_ms": round(avg_ms, 4),
+                "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in ktimes.items()}}
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tr = json.load(f).get(top_name)
+        if tr:
+            roofline["traffic"] = tr.get("bytes_per_launch")
+            roofline["traffic_source"] = tr.get("source")
+
+    # ---------------- end to end through the C ABI (e2e) ----------------
+    nthreads = args.e2e_threads
+    pinned = []
+    host_pairs = []
+    for p1, p2, _ in pairs:
+        bufs = []
+        for p in list(p1) + list(p2):
+            pb = api.PinnedBuffer(p.nbytes)
+            pb.array[:] = p.view(np.uint8).reshape(-1)
+            pinned.append(pb)
+            bufs.append(pb.ptr.value)
+        host_pairs.append((bufs[:3], bufs[3:]))
+    handlers = [api.SSIMU2(cs, gpu_id=local) for _ in range(nthreads)]
+    e2e_scores = np.zeros(BATCH)
+
+    def worker(k):
+        torch.cuda.set_device(local)
+        for i in range(k, BATCH, nthreads):
+            e2e_scores[i] = handlers[k].compute(host_pairs[i][0], host_pairs[i][1], ls, ls)
+
+    def e2e_step():
+        ths = [threading.Thread(target=worker, args=(k,)) for k in range(nthreads)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    e2e_value = BATCH * world * args.steps / e2e_s
+    max_dev = float(np.max(np.abs(e2e_scores - dev_scores)))
+    for hh in handlers:
+        hh.close()
+    h.close()
+    for pb in pinned:
+        pb.free()
+
+    # ---------------- CPU baseline: FP64 oracle on a bounded sample ----------------
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(pairs, cs, budget_s=args.cpu_seconds)
+        cpu["max_abs_dscore_vs_fp64"] = cpu.pop("_maxd", None)
+        # accuracy of our scores on the same sample against FP64
+        cpu_err = float(np.max(np.abs(np.array(cpu.pop("_scores")) - dev_scores[:cpu["_n"]])))
+        cpu.pop("_n")
+        cpu["max_abs_dscore_gpu_vs_fp64"] = cpu_err
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_step": BATCH, "width": W, "height": H,
+                   "format": "YUV420 10-bit limited BT.709", "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs (%.0f MB per step) larger than L2" % (input_bytes(pairs) / 1e6)},
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "api": "Vship_ComputeSSIMU2 (pinned host buffers)",
+                "threads_handlers": nthreads, "timer": "wall clock, synchronised",
+                "h2d_bytes_per_step": input_bytes(pairs), "d2h_bytes_per_step": BATCH * (8 + 108 * 4),
+                "max_abs_score_diff_vs_device_path": max_dev},
+        "gpu_launches": 3 * args.steps,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+    }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(pairs, cs, budget_s=12.0):
+    import oracle
+    oracle.build()
+    n, t0, scores, maxd = 0, time.perf_counter(), [], 0.0
+    while n < len(pairs) and (time.perf_counter() - t0) < budget_s:
+        p1, p2, ls = pairs[n]
+        q, d, _ = oracle.ssimu2(oracle.convert(p1, ls, cs), oracle.convert(p2, ls, cs))
+        scores.append(d)
+        maxd = max(maxd, abs(q - d))
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": round(n / dt, 3), "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+            "sample": "%d of the workload's 1080p pairs, colour conversion + SSIMU2 in FP64 (%.1f s)" % (n, dt),
+            "_scores": scores, "_n": n, "_maxd": maxd}
+
+
+def run_reference(args, world, rank, local):
+    if rank != 0:
+        return
+    from vship_b200 import abi, api
+    ref = os.path.join(ROOT, "oracle", "_ref", "libvship_ref.so")
+    if not os.path.exists(ref):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libvship_ref.so was not built"}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    L = api.load_library(ref)
+    cs = abi.yuv420_10bit_bt709(W, H)
+    pairs = make_workload(seed=1234)
+    ls = pairs[0][2]
+    pinned, host_pairs = [], []
+    for p1, p2, _ in pairs:
+        bufs = []
+        for p in list(p1) + list(p2):
+            pb = api.PinnedBuffer(p.nbytes, lib=L)
+            pb.array[:] = p.view(np.uint8).reshape(-1)
+            pinned.append(pb)
+            bufs.append(pb.ptr.value)
+        host_pairs.append((bufs[:3], bufs[3:]))
+    best = None
+    for nthreads in args.ref_threads:
+        handlers = [api.SSIMU2(cs, gpu_id=local, lib=L) for _ in range(nthreads)]
+        out = np.zeros(BATCH)
+
+        def worker(k):
+            torch.cuda.set_device(local)
+            for i in range(k, BATCH, nthreads):
+                out[i] = handlers[k].compute(host_pairs[i][0], host_pairs[i][1], ls, ls)
+
+        def step():
+            ths = [threading.Thread(target=worker, args=(k,)) for k in range(nthreads)]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        v = BATCH * args.steps / dt
+        log("reference: %d handlers/threads -> %.1f pairs/s" % (nthreads, v))
+        if best is None or v > best[0]:
+            best = (v, nthreads, dt)
+        for hh in handlers:
+            hh.close()
+    for pb in pinned:
+        pb.free()
+    v, nthreads, dt = best
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_step": BATCH, "width": W, "height": H,
+                   "format": "YUV420 10-bit limited BT.709",
+                   "library": "Vship 4.1.0 built from its sources with nvcc for sm_100a (oracle/build_ref.sh)",
+                   "api": "Vship_ComputeSSIMU2 with pinned host buffers", "threads_handlers": nthreads,
+                   "threads_swept": args.ref_threads},
+        "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "kind": "reference", "cores": nthreads,
+                         "sample": "%d steps of %d pairs; the reference has no CPU implementation, so its own CUDA "
+                                   "build runs on the B200, driven by %d host threads" % (args.steps, BATCH, nthreads)},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-threads", type=int, default=4)
+    ap.add_argument("--ref-threads", type=int, nargs="+", default=[1, 3, 4, 8])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank, local)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

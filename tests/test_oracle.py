@@ -1,0 +1,201 @@
+"""CPU tests of the FP64 oracle: known-answer checks of each stage, the reference's own
+identity invariant (test/libvshipTestIdentity.cpp:357-384, 444-453), and the pin against
+scores produced by the reference library itself on a B200 (tests/golden/)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from vship_b200 import abi, synth
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.json")
+
+
+def _rgb(oracle, planes, ls, cs):
+    return oracle.convert(planes, ls, cs)
+
+
+def test_identity_invariant(oracle_lib):
+    rng = np.random.default_rng(3)
+    img = rng.integers(0, 256, (3, 37, 53), dtype=np.uint8)
+    cs = abi.srgb8(53, 37)
+    rgb = oracle_lib.convert([img[c].tobytes() for c in range(3)], [53] * 3, cs)
+    q, d, f = oracle_lib.ssimu2(rgb, rgb)
+    assert q == 100.0
+    assert abs(d - 100.0) < 1e-6
+    norms, dmap = oracle_lib.butteraugli(rgb, rgb, 203.0, 5)
+    assert norms == (0.0, 0.0, 0.0)
+    assert np.all(dmap == 0.0)
+
+
+def test_blur_impulse_and_borders(oracle_lib):
+    # Interior impulse: separable normalised 17-tap Gaussian (src/ssimu2/gaussianblur.hpp:7-18).
+    x = np.zeros((40, 40))
+    x[20, 20] = 1.0
+    y = oracle_lib.blur(x, 1.5, 8)
+    g = np.exp(-((np.arange(17) - 8) ** 2) / (2 * 1.5 ** 2))
+    g /= g.sum()
+    np.testing.assert_allclose(y[12:29, 12:29], np.outer(g, g), rtol=1e-12, atol=1e-15)
+    # Renormalisation: a constant image stays constant everywhere, borders included.
+    c = np.full((13, 7), 0.37)
+    np.testing.assert_allclose(oracle_lib.blur(c, 1.5, 8), c, rtol=1e-14)
+    np.testing.assert_allclose(oracle_lib.blur(c, 7.15593339443, 21), c, rtol=1e-14)
+    # Corner impulse: weights over in-bounds taps only.
+    z = np.zeros((20, 20))
+    z[0, 0] = 1.0
+    n0 = g[8:].sum()
+    expect = np.array([g[8 - x] / g[8 - x:].sum() for x in range(9)]) * (g[8] / n0)
+    np.testing.assert_allclose(oracle_lib.blur(z, 1.5, 8)[0, :9], expect, rtol=1e-12)
+
+
+def test_downsample_odd_sizes(oracle_lib):
+    x = np.arange(35, dtype=np.float64).reshape(5, 7)
+    d = oracle_lib.downsample(x)
+    assert d.shape == (3, 4)
+    assert d[0, 0] == (0 + 1 + 7 + 8) / 4
+    assert d[2, 3] == x[4, 6]  # both axes clamp to the last sample
+    assert d[1, 3] == (x[2, 6] + x[3, 6]) / 2
+
+
+def test_final_score(oracle_lib):
+    f = np.zeros(108)
+    assert oracle_lib.ssimu2_final(f, True) == 100.0
+    rng = np.random.default_rng(0)
+    f = rng.uniform(0, 0.05, 108)
+    from tests.tables import weights
+    s = float(np.dot(weights(), f)) * 0.9562382616834844
+    s = 6.248496625763138e-5 * s ** 3 + 2.326765642916932 * s - 0.020884521182843837 * s * s
+    expect = 100.0 - 10.0 * s ** 0.6276336467831387 if s > 0 else 100.0
+    assert abs(oracle_lib.ssimu2_final(f, False) - expect) < 1e-9
+    # The float accumulation of the reference moves the score by float rounding only.
+    assert abs(oracle_lib.ssimu2_final(f, True) - expect) < 1e-3
+
+
+def test_pruned_features_are_zero(oracle_lib):
+    pairs = synth.make_pairs(1, 96, 64, fmt="rgb8", seed=5)
+    p1, p2, ls = pairs[0]
+    cs = abi.srgb8(96, 64)
+    _, _, f = oracle_lib.ssimu2(oracle_lib.convert(p1, ls, cs), oracle_lib.convert(p2, ls, cs))
+    from tests.tables import weights
+    w = weights()
+    for plane in range(3):
+        for scale in range(6):
+            for m in range(3):
+                on = w[plane * 36 + scale * 6 + m] > 0.01 or w[plane * 36 + scale * 6 + 3 + m] > 0.01
+                idx = [plane * 36 + scale * 6 + m, plane * 36 + scale * 6 + 3 + m]
+                if not on:
+                    assert f[idx[0]] == 0.0 and f[idx[1]] == 0.0
+    assert (f != 0).sum() > 0
+
+
+def test_colour_known_answers(oracle_lib):
+    # 8-bit full-range sRGB: 0 -> 0, 255 -> 1, knee value 10 (10/255 < 0.04045) is linear.
+    v = np.array([[0, 255, 10]], dtype=np.uint8)
+    cs = abi.srgb8(3, 1)
+    rgb = oracle_lib.convert([v.tobytes()] * 3, [3] * 3, cs)
+    np.testing.assert_allclose(rgb[0, 0], [0.0, 1.0, 10 / 255 / 12.92], rtol=1e-12)
+    # 10-bit limited BT.709: Y=64 -> black, Y=940 -> white (pure 2.4 gamma of 1 is 1).
+    cs = abi.yuv420_10bit_bt709(2, 2)
+    y = np.array([[64, 940], [64, 940]], dtype=np.uint16)
+    c = np.array([[512]], dtype=np.uint16)
+    rgb = oracle_lib.convert([y.tobytes(), c.tobytes(), c.tobytes()], [4, 2, 2], cs)
+    np.testing.assert_allclose(rgb[:, 0, 0], 0.0, atol=1e-12)
+    np.testing.assert_allclose(rgb[:, 0, 1], 1.0, rtol=1e-12)
+
+
+def test_high_bits_are_masked(oracle_lib):
+    # Garbage above the sample's bit depth is ignored (anyDepthToFloat.hpp:53-65).
+    cs = abi.colorspace(4, 1, sample=abi.SampleUINT10, range_=abi.RangeFull, family=abi.ColorRGB,
+                        matrix=abi.MATRIX_RGB, transfer=abi.TRC_Linear)
+    clean = np.array([[0, 100, 1023, 7]], dtype=np.uint16)
+    dirty = clean | np.array([[0xFC00, 0x8000, 0x0400, 0xF000]], dtype=np.uint16)
+    a = oracle_lib.convert([clean.tobytes()] * 3, [8] * 3, cs)
+    b = oracle_lib.convert([dirty.tobytes()] * 3, [8] * 3, cs)
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("subw,subh,loc", [(1, 1, abi.ChromaLoc_Left), (1, 1, abi.ChromaLoc_Center),
+                                           (2, 0, abi.ChromaLoc_Left), (2, 1, abi.ChromaLoc_Center),
+                                           (1, 0, abi.ChromaLoc_TopLeft), (0, 1, abi.ChromaLoc_Top)])
+def test_chroma_upsampling_reproduces_ramps(oracle_lib, subw, subh, loc):
+    # Cubic Hermite with central-difference tangents is exact on linear ramps away from the
+    # clamped edges; constant chroma stays constant everywhere.
+    W, H = 40, 24
+    cw, ch = ((W - 1) >> subw) + 1, ((H - 1) >> subh) + 1
+    cs = abi.colorspace(W, H, sample=abi.SampleUINT16, range_=abi.RangeFull, subw=subw, subh=subh,
+                        chroma_location=loc, family=abi.ColorRGB, matrix=abi.MATRIX_RGB, transfer=abi.TRC_Linear)
+    luma = np.zeros((H, W), np.uint16)
+    const = np.full((ch, cw), 40000, np.uint16)
+    rgb = oracle_lib.convert([luma.tobytes(), const.tobytes(), const.tobytes()], [2 * W, 2 * cw, 2 * cw], cs)
+    np.testing.assert_allclose(rgb[1], 40000 / 65535, rtol=1e-12)
+    ramp = (np.arange(cw)[None, :] * 300 + np.arange(ch)[:, None] * 200 + 1000).astype(np.uint16)
+    rgb = oracle_lib.convert([luma.tobytes(), ramp.tobytes(), ramp.tobytes()], [2 * W, 2 * cw, 2 * cw], cs)
+    f = 1 << subw
+    g = 1 << subh
+    cen_h = loc in (abi.ChromaLoc_Center, abi.ChromaLoc_Top)
+    cen_v = loc in (abi.ChromaLoc_Center, abi.ChromaLoc_Left)
+    xs = (np.arange(W) - ((f - 1) / 2 if cen_h and subw else 0)) / f
+    ys = (np.arange(H) - ((g - 1) / 2 if cen_v and subh else 0)) / g
+    expect = (xs[None, :] * 300 + ys[:, None] * 200 + 1000) / 65535
+    inner = (slice(2 * g, H - 3 * g), slice(2 * f, W - 3 * f))
+    np.testing.assert_allclose(rgb[1][inner], expect[inner], rtol=1e-12, atol=1e-12)
+
+
+def test_scores_decrease_with_distortion(oracle_lib):
+    rng = np.random.default_rng(11)
+    ref = synth.reference_rgb(rng, 128, 96)
+    cs = abi.srgb8(128, 96)
+    p1, ls = synth.to_rgb8(ref)
+    r1 = oracle_lib.convert(p1, ls, cs)
+    scores, butter = [], []
+    for step in (2, 12, 40):
+        p2, _ = synth.to_rgb8(synth.dct_quantize(ref, step))
+        r2 = oracle_lib.convert(p2, ls, cs)
+        scores.append(oracle_lib.ssimu2(r1, r2)[1])
+        butter.append(oracle_lib.butteraugli(r1, r2, 203.0, 5)[0][0])
+    assert scores[0] > scores[1] > scores[2]
+    assert butter[0] < butter[1] < butter[2]
+
+
+def _golden():
+    if not os.path.exists(GOLDEN):
+        pytest.skip("reference golden vectors not generated yet (tests/golden/make_golden.py on a GPU)")
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+def test_oracle_matches_reference_golden_ssimu2(oracle_lib):
+    from tests.golden.cases import build_case
+    data = _golden()
+    checked = 0
+    for case in data["cases"]:
+        if case["metric"] != "ssimu2" or case["w"] * case["h"] > 2_100_000:
+            continue
+        (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
+        q, d, _ = oracle_lib.ssimu2(oracle_lib.convert(p1, ls1, cs1), oracle_lib.convert(p2, ls2, cs2))
+        assert abs(q - case["score"]) <= 1e-3, (case["name"], q, case["score"])
+        checked += 1
+    assert checked >= 5
+
+
+def test_oracle_matches_reference_golden_butteraugli(oracle_lib):
+    from tests.golden.cases import build_case
+    data = _golden()
+    checked = 0
+    for case in data["cases"]:
+        if case["metric"] != "butteraugli" or case["w"] * case["h"] > 600_000:
+            continue
+        (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
+        norms, dmap = oracle_lib.butteraugli(oracle_lib.convert(p1, ls1, cs1), oracle_lib.convert(p2, ls2, cs2),
+                                             case["intensity"], case["qnorm"])
+        ref = case["norms"]
+        for k in range(3):
+            assert abs(norms[k] - ref[k]) <= 1e-4 * max(abs(ref[k]), 1e-6), (case["name"], k, norms, ref)
+        if "distmap_sample" in case:
+            idx = np.array(case["distmap_sample"]["index"])
+            val = np.array(case["distmap_sample"]["value"])
+            got = dmap.reshape(-1)[idx]
+            np.testing.assert_allclose(got, val, rtol=2e-4, atol=2e-6)
+        checked += 1
+    assert checked >= 3

@@ -1,0 +1,41 @@
+"""GPU parity against the reference itself: the unmodified Vship library, built from its own
+sources for sm_100a (oracle/_ref/libvship_ref.so), scores the same inputs in the same
+process through the same C ABI.  Tolerances as for the FP64 oracle: |dSSIMU2| <= 1e-3,
+Butteraugli norms within 1e-4 relative."""
+import os
+
+import pytest
+
+from tests.golden.cases import CASES, build_case
+from vship_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libvship_ref.so")
+
+
+@pytest.fixture(scope="module")
+def ref_lib(gpu):
+    if not os.path.exists(REF):
+        pytest.skip("reference library not built (oracle/build_ref.sh needs the reference sources)")
+    return api.load_library(REF)
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["w"] * c["h"] <= 2_100_000], ids=lambda c: c["name"])
+def test_matches_reference_library(gpu, ref_lib, case):
+    (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
+    if case["metric"] == "ssimu2":
+        with api.SSIMU2(cs1, cs2) as mine:
+            a = mine.compute(p1, p2, ls1, ls2)
+        ref = api.SSIMU2(cs1, cs2, lib=ref_lib)
+        b = ref.compute(p1, p2, ls1, ls2)
+        ref.close()
+        assert abs(a - b) <= 1e-3, (a, b)
+    else:
+        with api.Butteraugli(cs1, cs2, qnorm=case["qnorm"], intensity=case["intensity"]) as mine:
+            a, _ = mine.compute(p1, p2, ls1, ls2)
+        ref = api.Butteraugli(cs1, cs2, qnorm=case["qnorm"], intensity=case["intensity"], lib=ref_lib)
+        b, _ = ref.compute(p1, p2, ls1, ls2)
+        ref.close()
+        for k in range(3):
+            assert abs(a[k] - b[k]) <= 1e-4 * max(abs(b[k]), 1e-12), (k, a, b)

@@ -1,0 +1,108 @@
+"""GPU parity of the SSIMULACRA2 path through the C ABI against the FP64 oracle.
+
+Tolerance: |dSSIMU2| <= 1e-3 against FP64 (the accuracy bar of the engine); features within
+1e-4 relative.  Identical inputs must give exactly 100, as the reference's identity test
+requires (test/libvshipTestIdentity.cpp:357-384).
+"""
+import numpy as np
+import pytest
+
+from tests.golden.cases import CASES, build_case
+from vship_b200 import abi, api, synth
+
+pytestmark = pytest.mark.gpu
+
+SCORE_TOL = 1e-3
+
+
+def _oracle_score(oracle, a, b):
+    (p1, ls1, cs1), (p2, ls2, cs2) = a, b
+    return oracle.ssimu2(oracle.convert(p1, ls1, cs1), oracle.convert(p2, ls2, cs2))
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["metric"] == "ssimu2"], ids=lambda c: c["name"])
+def test_cases_match_oracle(gpu, oracle_lib, case):
+    a, b = build_case(case)
+    with api.SSIMU2(a[2], b[2]) as h:
+        got = h.compute(a[0], b[0], a[1], b[1])
+        feats = h.last_features()
+    q, d, f = _oracle_score(oracle_lib, a, b)
+    if case.get("identical"):
+        assert got == 100.0
+        return
+    assert abs(got - d) <= SCORE_TOL, (got, d)
+    np.testing.assert_allclose(feats, f, rtol=1e-4, atol=2e-6)
+
+
+@pytest.mark.parametrize("fmt,w,h", [("rgb8", 64, 64), ("yuv420p10", 130, 98), ("rgb8", 1920, 1080)])
+def test_identity_exact(gpu, fmt, w, h):
+    p1, _, ls = synth.make_pairs(1, w, h, fmt=fmt, seed=9)[0]
+    cs = abi.srgb8(w, h) if fmt == "rgb8" else abi.yuv420_10bit_bt709(w, h)
+    padded, pls = synth.with_padding(p1, ls, [13, 5, 9])
+    with api.SSIMU2(cs) as hd:
+        assert hd.compute(p1, padded, ls, pls) == 100.0
+
+
+def test_1080p_workloads(gpu, oracle_lib):
+    for fmt, cs in (("rgb8", abi.srgb8(1920, 1080)), ("yuv420p10", abi.yuv420_10bit_bt709(1920, 1080))):
+        pairs = synth.make_pairs(2, 1920, 1080, fmt=fmt, seed=21)
+        with api.SSIMU2(cs) as h:
+            for p1, p2, ls in pairs:
+                got = h.compute(p1, p2, ls)
+                _, d, _ = oracle_lib.ssimu2(oracle_lib.convert(p1, ls, cs), oracle_lib.convert(p2, ls, cs))
+                assert abs(got - d) <= SCORE_TOL, (fmt, got, d)
+
+
+def test_device_batch_matches_host_api(gpu):
+    import torch
+    w, h = 640, 360
+    pairs = synth.make_pairs(5, w, h, fmt="yuv420p10", seed=4, unique=2)
+    cs = abi.yuv420_10bit_bt709(w, h)
+    with api.SSIMU2(cs) as hd:
+        host = [hd.compute(p1, p2, ls) for p1, p2, ls in pairs]
+        dev = [([torch.from_numpy(p.view(np.uint8).copy()).cuda() for p in p1],
+                [torch.from_numpy(p.view(np.uint8).copy()).cuda() for p in p2]) for p1, p2, _ in pairs]
+        ptr1 = [t.data_ptr() for d in dev for t in d[0]]
+        ptr2 = [t.data_ptr() for d in dev for t in d[1]]
+        scores = torch.zeros(len(pairs), dtype=torch.float64, device="cuda")
+        feats = torch.zeros(len(pairs), 108, dtype=torch.float32, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        hd.compute_device(len(pairs), ptr1, ptr2, pairs[0][2], pairs[0][2], scores.data_ptr(), feats.data_ptr(), stream)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(scores.cpu().numpy(), np.array(host))
+        assert torch.all(feats.sum(dim=1) > 0)
+
+
+def test_device_api_strided_and_misaligned(gpu):
+    import torch
+    w, h = 97, 61
+    cs = abi.colorspace(w, h, sample=abi.SampleUINT16, range_=abi.RangeFull, family=abi.ColorRGB,
+                        matrix=abi.MATRIX_RGB, transfer=abi.TRC_sRGB)
+    rng = np.random.default_rng(2)
+    planes = [rng.integers(0, 65536, (h, w), dtype=np.uint16) for _ in range(3)]
+    dist = [np.clip(p.astype(np.int64) + rng.integers(-900, 900, p.shape), 0, 65535).astype(np.uint16) for p in planes]
+    with api.SSIMU2(cs) as hd:
+        ref = hd.compute(planes, dist, [2 * w] * 3)
+        # odd byte strides force the byte-wise sample loads
+        pp, pls = synth.with_padding(planes, [2 * w] * 3, [3, 5, 7])
+        dd, dls = synth.with_padding(dist, [2 * w] * 3, [1, 1, 1])
+        d1 = [torch.from_numpy(p).cuda() for p in pp]
+        d2 = [torch.from_numpy(p).cuda() for p in dd]
+        s = torch.zeros(1, dtype=torch.float64, device="cuda")
+        hd.compute_device(1, [t.data_ptr() for t in d1], [t.data_ptr() for t in d2], pls, dls, s.data_ptr())
+        torch.cuda.synchronize()
+        assert abs(s.item() - ref) <= 1e-9
+
+
+def test_errors(gpu):
+    cs1, cs2 = abi.srgb8(64, 64), abi.srgb8(64, 65)
+    with pytest.raises(api.VshipError) as e:
+        api.SSIMU2(cs1, cs2)
+    assert e.value.code == abi.DifferingInputType
+    assert "DifferingInputType" in str(e.value)
+    with api.SSIMU2(cs1) as h:
+        p = [np.zeros((64, 64), np.uint8)] * 3
+        with pytest.raises(api.VshipError) as e:
+            h.compute(p, p, [32, 64, 64])
+        assert e.value.code == abi.BadPointer
+        assert h.compute(p, p, [64] * 3) == 100.0

@@ -1,0 +1,299 @@
+"""Python binding of libvship.so (the B200 engine behind Vship's C ABI).
+
+Loads the in-tree library with ctypes and mirrors the reference's API surface
+(src/VshipAPI.h): handler objects for SSIMULACRA2 and Butteraugli with the same argument
+meaning and the same error codes, raised here as VshipError carrying the library's detailed
+message.  It refuses to run without the compiled library: there is no Python or CPU fallback.
+"""
+import ctypes
+import os
+import threading
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvship.so")
+
+_lib = None
+_lock = threading.Lock()
+
+
+class VshipError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+        self.name = abi.EXCEPTIONS.get(code, "BadErrorType")
+
+
+def _declare(L):
+    c = ctypes
+    H2, HB = abi.SSIMU2Handler, abi.ButteraugliHandler
+    u8pp = c.POINTER(c.POINTER(c.c_uint8))
+    i64p = c.POINTER(c.c_int64)
+    L.Vship_GetVersion.restype = abi.Version
+    L.Vship_GetVersion.argtypes = []
+    L.Vship_GetDeviceCount.argtypes = [c.POINTER(c.c_int)]
+    L.Vship_SetDevice.argtypes = [c.c_int]
+    L.Vship_GetDeviceInfo.argtypes = [c.POINTER(abi.DeviceInfo), c.c_int]
+    L.Vship_GPUFullCheck.argtypes = [c.c_int]
+    L.Vship_GetErrorMessage.argtypes = [c.c_int, c.c_char_p, c.c_int]
+    L.Vship_GetErrorMessage.restype = c.c_int
+    L.Vship_GetDetailedLastError.argtypes = [c.c_char_p, c.c_int]
+    L.Vship_GetDetailedLastError.restype = c.c_int
+    L.Vship_PinnedMalloc.argtypes = [c.POINTER(c.c_void_p), c.c_uint64]
+    L.Vship_PinnedFree.argtypes = [c.c_void_p]
+    L.Vship_SSIMU2Init.argtypes = [c.POINTER(H2), abi.Colorspace, abi.Colorspace]
+    L.Vship_SSIMU2Init2.argtypes = [c.POINTER(H2), abi.Colorspace, abi.Colorspace, c.c_int]
+    L.Vship_SSIMU2Free.argtypes = [H2]
+    L.Vship_ComputeSSIMU2.argtypes = [H2, c.POINTER(c.c_double), u8pp, u8pp, i64p, i64p]
+    L.Vship_SSIMU2GetDetailedLastError.argtypes = [H2, c.c_char_p, c.c_int]
+    L.Vship_SSIMU2GetDetailedLastError.restype = c.c_int
+    L.Vship_ButteraugliInit.argtypes = [c.POINTER(HB), abi.Colorspace, abi.Colorspace, c.c_int, c.c_float]
+    L.Vship_ButteraugliInit2.argtypes = [c.POINTER(HB), abi.Colorspace, abi.Colorspace, c.c_int, c.c_float, c.c_int]
+    L.Vship_ButteraugliFree.argtypes = [HB]
+    L.Vship_ComputeButteraugli.argtypes = [HB, c.POINTER(abi.ButteraugliScore), c.c_void_p, c.c_int64, u8pp, u8pp, i64p, i64p]
+    L.Vship_ButteraugliGetDetailedLastError.argtypes = [HB, c.c_char_p, c.c_int]
+    L.Vship_ButteraugliGetDetailedLastError.restype = c.c_int
+    # extensions
+    vpp = c.POINTER(c.c_void_p)
+    L.VshipExt_ComputeSSIMU2Device.argtypes = [H2, c.c_int, c.c_void_p, c.c_void_p, vpp, vpp, i64p, i64p, c.c_void_p]
+    L.VshipExt_SSIMU2LastFeatures.argtypes = [H2, c.POINTER(c.c_float)]
+    L.VshipExt_ComputeButteraugliDevice.argtypes = [HB, c.c_void_p, c.c_void_p, c.c_int64, vpp, vpp, i64p, i64p, c.c_void_p]
+    L.VshipExt_SSIMU2KernelTiming.argtypes = [H2, c.c_int]
+    L.VshipExt_SSIMU2KernelTimes.argtypes = [H2, c.c_void_p, c.c_int, c.c_int]
+    L.VshipExt_SSIMU2KernelTimes.restype = c.c_int
+    L.VshipExt_ButteraugliKernelTiming.argtypes = [HB, c.c_int]
+    L.VshipExt_ButteraugliKernelTimes.argtypes = [HB, c.c_void_p, c.c_int, c.c_int]
+    L.VshipExt_ButteraugliKernelTimes.restype = c.c_int
+    L.VshipExt_SSIMU2Resolution.argtypes = [H2, i64p, i64p]
+    L.VshipExt_ButteraugliResolution.argtypes = [HB, i64p, i64p]
+    return L
+
+
+class KernelTime(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_int), ("total_ms", ctypes.c_double)]
+
+
+def load(path=None):
+    """Loads (once) and returns the ctypes handle of libvship.so; raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is None or path is not None:
+            p = path or LIB_PATH
+            if not os.path.exists(p):
+                raise RuntimeError("libvship.so is not built (run `python -m vship_b200.build`): %s" % p)
+            _lib = _declare(ctypes.CDLL(p))
+        return _lib
+
+
+def load_library(path):
+    """A separate handle on any library exporting the Vship ABI (e.g. the reference build)."""
+    return _declare(ctypes.CDLL(path))
+
+
+def _message(L, fn=None, handler=None):
+    if fn is None:
+        n = L.Vship_GetDetailedLastError(None, 0)
+        buf = ctypes.create_string_buffer(n)
+        L.Vship_GetDetailedLastError(buf, n)
+    else:
+        n = fn(handler, None, 0)
+        if n <= 0:
+            return _message(L)
+        buf = ctypes.create_string_buffer(n)
+        fn(handler, buf, n)
+    return buf.value.decode(errors="replace")
+
+
+def check(L, rc, fn=None, handler=None):
+    if rc != 0:
+        raise VshipError(rc, _message(L, fn, handler))
+
+
+def planes_arg(planes):
+    """Three buffers (bytes / numpy / ctypes addresses) -> uint8_t*[3] and keep-alive list."""
+    keep = []
+    arr = abi.PlanePtrs()
+    for i, p in enumerate(planes):
+        if isinstance(p, int):
+            arr[i] = ctypes.cast(ctypes.c_void_p(p), ctypes.POINTER(ctypes.c_uint8))
+            continue
+        if hasattr(p, "ctypes"):
+            addr = p.ctypes.data
+            keep.append(p)
+        else:
+            buf = (ctypes.c_uint8 * len(p)).from_buffer_copy(p)
+            keep.append(buf)
+            addr = ctypes.addressof(buf)
+        arr[i] = ctypes.cast(ctypes.c_void_p(addr), ctypes.POINTER(ctypes.c_uint8))
+    return arr, keep
+
+
+def version(lib=None):
+    v = (lib or load()).Vship_GetVersion()
+    return (v.major, v.minor, v.minorMinor, v.backend)
+
+
+def device_count(lib=None):
+    L = lib or load()
+    n = ctypes.c_int(0)
+    check(L, L.Vship_GetDeviceCount(ctypes.byref(n)))
+    return n.value
+
+
+def error_message(code, lib=None):
+    L = lib or load()
+    n = L.Vship_GetErrorMessage(code, None, 0)
+    buf = ctypes.create_string_buffer(n)
+    L.Vship_GetErrorMessage(code, buf, n)
+    return buf.value.decode()
+
+
+class SSIMU2:
+    """An SSIMULACRA2 handler (Vship_SSIMU2Init2 .. Vship_SSIMU2Free)."""
+
+    def __init__(self, src_cs, dis_cs=None, gpu_id=0, lib=None):
+        self.L = lib or load()
+        self.h = abi.SSIMU2Handler()
+        self.src_cs, self.dis_cs = src_cs, dis_cs or src_cs
+        rc = self.L.Vship_SSIMU2Init2(ctypes.byref(self.h), self.src_cs, self.dis_cs, gpu_id)
+        self.alive = True
+        if rc != 0:
+            msg = _message(self.L, self.L.Vship_SSIMU2GetDetailedLastError, self.h)
+            self.close()
+            raise VshipError(rc, msg)
+
+    def compute(self, planes1, planes2, line_sizes1, line_sizes2=None):
+        a1, k1 = planes_arg(planes1)
+        a2, k2 = planes_arg(planes2)
+        ls1 = abi.LineSizes(*line_sizes1)
+        ls2 = abi.LineSizes(*(line_sizes2 or line_sizes1))
+        score = ctypes.c_double()
+        rc = self.L.Vship_ComputeSSIMU2(self.h, ctypes.byref(score), a1, a2, ls1, ls2)
+        check(self.L, rc, self.L.Vship_SSIMU2GetDetailedLastError, self.h)
+        return score.value
+
+    def last_features(self):
+        import numpy as np
+        out = (ctypes.c_float * 108)()
+        check(self.L, self.L.VshipExt_SSIMU2LastFeatures(self.h, out))
+        return np.frombuffer(out, dtype=np.float32).copy()
+
+    def compute_device(self, n, ptrs1, ptrs2, line_sizes1, line_sizes2, d_scores, d_features=0, stream=0):
+        """ptrs1/ptrs2: 3*n device plane addresses; d_scores/d_features: device addresses."""
+        a1 = (ctypes.c_void_p * (3 * n))(*ptrs1)
+        a2 = (ctypes.c_void_p * (3 * n))(*ptrs2)
+        rc = self.L.VshipExt_ComputeSSIMU2Device(self.h, n, d_scores, d_features or None, a1, a2,
+                                                 abi.LineSizes(*line_sizes1), abi.LineSizes(*line_sizes2), stream or None)
+        check(self.L, rc, self.L.Vship_SSIMU2GetDetailedLastError, self.h)
+
+    def kernel_timing(self, enable=True):
+        check(self.L, self.L.VshipExt_SSIMU2KernelTiming(self.h, 1 if enable else 0))
+
+    def kernel_times(self, reset=False):
+        out = (KernelTime * 8)()
+        n = self.L.VshipExt_SSIMU2KernelTimes(self.h, out, 8, 1 if reset else 0)
+        if n < 0:
+            check(self.L, abi.BadHandler)
+        return {out[i].name.decode(): (out[i].launches, out[i].total_ms) for i in range(n)}
+
+    def close(self):
+        if getattr(self, "alive", False):
+            self.alive = False
+            self.L.Vship_SSIMU2Free(self.h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Butteraugli:
+    """A Butteraugli handler (Vship_ButteraugliInit2 .. Vship_ButteraugliFree)."""
+
+    def __init__(self, src_cs, dis_cs=None, qnorm=2, intensity=203.0, gpu_id=0, lib=None):
+        self.L = lib or load()
+        self.h = abi.ButteraugliHandler()
+        self.src_cs, self.dis_cs = src_cs, dis_cs or src_cs
+        rc = self.L.Vship_ButteraugliInit2(ctypes.byref(self.h), self.src_cs, self.dis_cs, int(qnorm), float(intensity), gpu_id)
+        self.alive = True
+        if rc != 0:
+            msg = _message(self.L, self.L.Vship_ButteraugliGetDetailedLastError, self.h)
+            self.close()
+            raise VshipError(rc, msg)
+
+    def compute(self, planes1, planes2, line_sizes1, line_sizes2=None, distmap=False):
+        """Returns ((normQ, norm3, norminf), distmap float32 (H, W) or None)."""
+        import numpy as np
+        a1, k1 = planes_arg(planes1)
+        a2, k2 = planes_arg(planes2)
+        ls1 = abi.LineSizes(*line_sizes1)
+        ls2 = abi.LineSizes(*(line_sizes2 or line_sizes1))
+        score = abi.ButteraugliScore()
+        dm = None
+        dst, stride = None, 0
+        if distmap:
+            w, h = self.src_cs.out_dims()
+            dm = np.zeros((h, w), dtype=np.float32)
+            dst, stride = dm.ctypes.data, w * 4
+        rc = self.L.Vship_ComputeButteraugli(self.h, ctypes.byref(score), dst, stride, a1, a2, ls1, ls2)
+        check(self.L, rc, self.L.Vship_ButteraugliGetDetailedLastError, self.h)
+        return (score.normQ, score.norm3, score.norminf), dm
+
+    def compute_device(self, ptrs1, ptrs2, line_sizes1, line_sizes2, d_norms, d_distmap=0, dststride=0, stream=0):
+        a1 = (ctypes.c_void_p * 3)(*ptrs1)
+        a2 = (ctypes.c_void_p * 3)(*ptrs2)
+        rc = self.L.VshipExt_ComputeButteraugliDevice(self.h, d_norms, d_distmap or None, dststride, a1, a2,
+                                                      abi.LineSizes(*line_sizes1), abi.LineSizes(*line_sizes2), stream or None)
+        check(self.L, rc, self.L.Vship_ButteraugliGetDetailedLastError, self.h)
+
+    def kernel_timing(self, enable=True):
+        check(self.L, self.L.VshipExt_ButteraugliKernelTiming(self.h, 1 if enable else 0))
+
+    def kernel_times(self, reset=False):
+        out = (KernelTime * 8)()
+        n = self.L.VshipExt_ButteraugliKernelTimes(self.h, out, 8, 1 if reset else 0)
+        if n < 0:
+            check(self.L, abi.BadHandler)
+        return {out[i].name.decode(): (out[i].launches, out[i].total_ms) for i in range(n)}
+
+    def close(self):
+        if getattr(self, "alive", False):
+            self.alive = False
+            self.L.Vship_ButteraugliFree(self.h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PinnedBuffer:
+    """Page-locked host memory from Vship_PinnedMalloc, exposed as a numpy uint8 array."""
+
+    def __init__(self, nbytes, lib=None):
+        import numpy as np
+        self.L = lib or load()
+        self.ptr = ctypes.c_void_p()
+        check(self.L, self.L.Vship_PinnedMalloc(ctypes.byref(self.ptr), nbytes))
+        self.nbytes = nbytes
+        self.array = np.ctypeslib.as_array((ctypes.c_uint8 * nbytes).from_address(self.ptr.value))
+
+    def free(self):
+        if self.ptr:
+            self.L.Vship_PinnedFree(self.ptr)
+            self.ptr = ctypes.c_void_p()

@@ -1,0 +1,277 @@
+// Colour front-end shared by both metrics: raw planes of any Vship_Colorspace_t -> linear
+// BT.709 RGB in FP32, one pixel at a time, fused into the consumers (the SSIMULACRA2 pyramid
+// kernel and the Butteraugli opsin kernel) so the intermediate float planes the reference
+// materialises (src/gpuColorToLinear/vshipColor.hpp:62-146) never touch HBM.
+//
+// Arithmetic follows the reference stage by stage, including its float/double promotions,
+// so that results agree to float rounding:
+//   sample decode      src/gpuColorToLinear/anyDepthToFloat.hpp:24-68
+//   range              src/gpuColorToLinear/rangeToFull.hpp:24-55
+//   chroma upsampling  src/gpuColorToLinear/chromaUpsample.hpp:28-247 (cubic Hermite)
+//   Y'CbCr -> R'G'B'   src/gpuColorToLinear/YUVToLinRGB.hpp:7-163
+//   transfer           src/gpuColorToLinear/transferToLinear.hpp:19-184
+//   primaries          src/gpuColorToLinear/primaries.hpp:9-158
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cstdint>
+
+#include "../../include/VshipColor.h"
+
+namespace vship {
+
+// Per-clip conversion parameters, resolved on the host at Init.
+struct ColourParams {
+    int sample;          // Vship_Sample_t
+    int bytes;           // bytes per stored sample
+    unsigned mask;       // low-bit mask for 16-bit integer containers
+    int misaligned;      // some stride is not a multiple of `bytes`: use byte loads
+    float full_norm;     // full range divisor (2^bits - 1, or 1 for float/half)
+    float lim_div;       // limited range: integer divisor 2^(bits-8) (0 for float/half)
+    int full_range;
+    int yuv_chroma;      // planes 1 and 2 are chroma (YUV family)
+    int subw, subh;
+    int hcenter, vcenter;
+    int matrix, trc, primaries;
+    int skip_yuv;        // Linear transfer + RGB matrix: no Y'CbCr/transfer stage
+    int64_t W, H;        // luma plane size
+    int64_t cw, ch;      // chroma plane size
+};
+
+// Device view of one input image: three plane base pointers and byte strides.
+struct RawImage {
+    const uint8_t* p[3];
+    int64_t stride[3];
+};
+
+__device__ __forceinline__ int64_t clamp64(int64_t v, int64_t lo, int64_t hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+// PickValue + FullRange for one stored sample.
+__device__ __forceinline__ float load_norm(const uint8_t* plane, int64_t stride, int64_t x, int64_t y,
+                                           const ColourParams& cp, bool chroma) {
+    const uint8_t* a = plane + y * stride + x * cp.bytes;
+    float v;
+    if (cp.sample == Vship_SampleUINT8) {
+        v = (float)__ldg(a);
+    } else if (cp.sample == Vship_SampleFLOAT) {
+        if (cp.misaligned) {
+            uint32_t u = (uint32_t)__ldg(a) | ((uint32_t)__ldg(a + 1) << 8) | ((uint32_t)__ldg(a + 2) << 16) | ((uint32_t)__ldg(a + 3) << 24);
+            v = __uint_as_float(u);
+        } else {
+            v = __ldg(reinterpret_cast<const float*>(a));
+        }
+    } else {
+        unsigned short u;
+        if (cp.misaligned) u = (unsigned short)(__ldg(a) | (__ldg(a + 1) << 8));
+        else u = __ldg(reinterpret_cast<const unsigned short*>(a));
+        if (cp.sample == Vship_SampleHALF) v = __half2float(__ushort_as_half(u));
+        else v = (float)(u & cp.mask);
+    }
+    if (cp.full_range) {
+        v /= cp.full_norm;
+        if (chroma) v -= 0.5f;
+        return v;
+    }
+    if (cp.lim_div > 0.f) v /= cp.lim_div;
+    else v *= 256.f;
+    return chroma ? (v - 128.f) / 224.f : (v - 16.f) / 219.f;
+}
+
+// CubicHermitSplineInterpolator (src/gpuColorToLinear/resize.hpp:5-24).
+__device__ __forceinline__ float hermite(float p0, float m0, float p1, float m1, float t) {
+    const float v1 = 2 * p0 + m0 - 2 * p1 + m1;
+    const float v2 = -3 * p0 + 3 * p1 - 2 * m0 - m1;
+    float r = v1;
+    r *= t; r += v2;
+    r *= t; r += m0;
+    r *= t; r += p0;
+    return r;
+}
+
+// Output sample X of an axis decimated by 2^sub -> interval start i and fraction t.
+// Co-sited (Left/Top) kernels put sample i at X = f*i; centred ones at X = f*i + (f-1)/2.
+__device__ __forceinline__ void upsample_phase(int64_t X, int sub, int centered, int64_t& i, float& t) {
+    if (sub == 0) { i = X; t = 0.f; return; }
+    const int64_t f = (int64_t)1 << sub;
+    if (!centered) {
+        i = X >> sub;
+        t = (float)(X & (f - 1)) / (float)f;
+    } else {
+        const int64_t off = X - f / 2;
+        const int64_t q = off >= 0 ? (off >> sub) : -((-off + f - 1) >> sub);
+        i = q;
+        t = ((float)(off - q * f) + 0.5f) / (float)f;
+    }
+}
+
+// Chroma plane c (1 or 2) upsampled to luma position (X, Y): horizontal Hermite on up to
+// four clamped chroma rows, then vertical Hermite (the reference's two passes, fused).
+__device__ __forceinline__ float chroma_at(const RawImage& im, int c, int64_t X, int64_t Y, const ColourParams& cp) {
+    const bool chroma = cp.yuv_chroma != 0;
+    const uint8_t* pl = im.p[c];
+    const int64_t st = im.stride[c];
+    if (cp.subw == 0 && cp.subh == 0) return load_norm(pl, st, X, Y, cp, chroma);
+    int64_t ix, iy;
+    float tx, ty;
+    upsample_phase(X, cp.subw, cp.hcenter, ix, tx);
+    upsample_phase(Y, cp.subh, cp.vcenter, iy, ty);
+    const int64_t c0 = clamp64(ix - 1, 0, cp.cw - 1), c1 = clamp64(ix, 0, cp.cw - 1);
+    const int64_t c2 = clamp64(ix + 1, 0, cp.cw - 1), c3 = clamp64(ix + 2, 0, cp.cw - 1);
+    auto hrow = [&](int64_t r) -> float {
+        if (cp.subw == 0) return load_norm(pl, st, X, r, cp, chroma);
+        const float em1 = load_norm(pl, st, c0, r, cp, chroma);
+        const float e0 = load_norm(pl, st, c1, r, cp, chroma);
+        const float e1 = load_norm(pl, st, c2, r, cp, chroma);
+        const float e2 = load_norm(pl, st, c3, r, cp, chroma);
+        return hermite(e0, (e1 - em1) / 2, e1, (e2 - e0) / 2, tx);
+    };
+    if (cp.subh == 0) return hrow(Y);
+    const float h0 = hrow(clamp64(iy - 1, 0, cp.ch - 1));
+    const float h1 = hrow(clamp64(iy, 0, cp.ch - 1));
+    const float h2 = hrow(clamp64(iy + 1, 0, cp.ch - 1));
+    const float h3 = hrow(clamp64(iy + 2, 0, cp.ch - 1));
+    return hermite(h1, (h2 - h0) / 2, h2, (h3 - h1) / 2, ty);
+}
+
+// Non-constant-luminance Y'CbCr -> R'G'B' (YUVToLinRGB.hpp:7-18).
+__device__ __forceinline__ float3 ncl_to_rgb(float3 v, const float kr, const float kb) {
+    const float kg = 1.f - kb - kr;
+    const float us = 0.5f / (1.f - kb);
+    const float vs = 0.5f / (1.f - kr);
+    float3 r;
+    r.x = (v.z + v.x * vs) / (vs * kr + 0.5f);
+    r.z = (v.y + v.x * us) / (us * kb + 0.5f);
+    r.y = (v.x - kr * r.x - kb * r.z) / kg;
+    return r;
+}
+
+__device__ __forceinline__ float3 gamma_light(float3 v, int matrix) {
+    switch (matrix) {
+    case Vship_MATRIX_BT709: return ncl_to_rgb(v, 0.2126f, 0.0722f);
+    case Vship_MATRIX_BT470_BG:
+    case Vship_MATRIX_ST170_M: return ncl_to_rgb(v, 0.299f, 0.114f);
+    case Vship_MATRIX_BT2020_NCL: return ncl_to_rgb(v, 0.2627f, 0.0593f);
+    case Vship_MATRIX_BT2020_CL: {
+        const float kr = 0.2627f, kb = 0.0593f;
+        const float us = 0.5f / (1.f - kb), vs = 0.5f / (1.f - kr);
+        float3 r;
+        r.x = (v.z + v.x * vs) / (vs * kr + 0.5f);
+        r.z = (v.y + v.x * us) / (us * kb + 0.5f);
+        r.y = v.x;
+        return r;
+    }
+    case Vship_MATRIX_BT2100_ICTCP:
+        v.x = fmaf(v.y, 0.0086090370379327566f, fmaf(v.z, 0.11102962500302595655f, v.x));
+        v.y = fmaf(v.y, -0.01721807407586551f, fmaf(v.z, -0.22205925000605192f, v.x));
+        v.z = fmaf(v.x, 33.025782688766114f, fmaf(v.y, -32.025782688766114f, -v.z * 7.543278084714549f));
+        return v;
+    default: return v;
+    }
+}
+
+__device__ __forceinline__ float3 linear_light(float3 v, int matrix) {
+    if (matrix == Vship_MATRIX_BT2020_CL) {
+        const float kr = 0.2627f, kb = 0.0593f, kg = 1.f - kr - kb;
+        v.y = (v.y - kr * v.x - kb * v.z) / kg;
+    } else if (matrix == Vship_MATRIX_BT2100_ICTCP) {
+        v.x = fmaf(v.x, 3.4366066943330784267f, fmaf(v.y, -2.5064521186562698975f, v.z * 0.069845424323191470954f));
+        v.y = fmaf(v.x, -0.23026480071281397f, fmaf(v.y, 1.4064527541936944f, -v.z * 0.2083538389058436f));
+        v.z = fmaf(v.x, -0.02684381778741865f, fmaf(v.y, -0.08378524945770065f, (float)((double)v.z * 1.106879231557486)));
+    }
+    return v;
+}
+
+__device__ __forceinline__ float signed_powf(float a, float g) { return a < 0 ? -powf(-a, g) : powf(a, g); }
+
+__device__ __forceinline__ float trc_one(float a, int trc) {
+    switch (trc) {
+    case Vship_TRC_sRGB:
+        if (a < 0) {
+            if (a < -0.04045f) return -powf((float)((-(double)a + 0.055) * (1.0 / 1.055)), 2.4f);
+            return (float)((double)a * (1.0 / 12.92));
+        }
+        if (a > 0.04045f) return powf((float)(((double)a + 0.055) * (1.0 / 1.055)), 2.4f);
+        return (float)((double)a * (1.0 / 12.92));
+    case Vship_TRC_BT709: return signed_powf(a, 2.4f);
+    case Vship_TRC_BT470_M: return signed_powf(a, 2.2f);
+    case Vship_TRC_BT470_BG:
+    case Vship_TRC_BT601: return signed_powf(a, 2.8f);
+    case Vship_TRC_ST240_M:
+        if (a >= 0) return a < 0.0228f ? 4 * a : (float)((double)(1.1115f * powf(a, 0.45f)) - 0.1115);
+        return a > -0.0228f ? 4 * a : (float)((double)(-1.1115f * powf(-a, 0.45f)) + 0.1115);
+    case Vship_TRC_ST428: return (float)((double)signed_powf(a, 2.6f) * (52.37 / 48.));
+    case Vship_TRC_PQ: {
+        const float m = 78.843750000000000f, n = 0.15930175781250000f;
+        const float c1 = 0.83593750000000000f, c2 = 18.851562500000000f, c3 = 18.687500000000000f;
+        a = fmaxf(0.f, a);
+        a = powf(a, 1.f / m);
+        return 100.f * powf(fmaxf(0.f, a - c1) / (c2 - c3 * a), 1.f / n);
+    }
+    default: return a;
+    }
+}
+
+__device__ __forceinline__ float3 transfer(float3 v, int trc) {
+    if (trc == Vship_TRC_HLG) {
+        const float a = 0.17883277f, b = 1.f - 4.f * a, c = 0.5f - a * -0.3350097945111627f;
+        v.x = v.x <= 0.5f ? v.x * v.x / 3.f : (expf((v.x - c) / a) + b) / 12.f;
+        v.y = v.y <= 0.5f ? v.y * v.y / 3.f : (expf((v.y - c) / a) + b) / 12.f;
+        v.z = v.z <= 0.5f ? v.z * v.z / 3.f : (expf((v.z - c) / a) + b) / 12.f;
+        const float ys = (float)((double)(0.2627f * v.x + 0.6780f * v.y) + 0.0593 * (double)v.z);
+        const float s = powf(ys, 1.2f - 1.f);
+        v.x *= s; v.y *= s; v.z *= s;
+        return v;
+    }
+    v.x = trc_one(v.x, trc);
+    v.y = trc_one(v.y, trc);
+    v.z = trc_one(v.z, trc);
+    return v;
+}
+
+__device__ __forceinline__ float3 mat3f(float3 a, float m0, float m1, float m2, float m3, float m4, float m5,
+                                        float m6, float m7, float m8) {
+    float3 r;
+    r.x = fmaf(a.x, m0, fmaf(a.y, m1, a.z * m2));
+    r.y = fmaf(a.x, m3, fmaf(a.y, m4, a.z * m5));
+    r.z = fmaf(a.x, m6, fmaf(a.y, m7, a.z * m8));
+    return r;
+}
+
+// Any supported primaries -> BT.709, through XYZ except for the direct BT.2020 matrix.
+__device__ __forceinline__ float3 primaries_to_709(float3 v, int prim) {
+    switch (prim) {
+    case Vship_PRIMARIES_BT709: return v;
+    case Vship_PRIMARIES_BT2020:
+        return mat3f(v, 1.6605f, -0.5876f, -0.0728f, -0.1246f, 1.1329f, -0.0083f, -0.0182f, -0.1006f, 1.1187f);
+    case Vship_PRIMARIES_ST170_M:
+    case Vship_PRIMARIES_ST240_M:
+        v = mat3f(v, 0.39349893f, 0.3652766f, 0.19162447f, 0.2123645f, 0.70109542f, 0.08654008f, 0.01873804f, 0.1119396f, 0.95812235f);
+        break;
+    case Vship_PRIMARIES_BT470_BG:
+        v = mat3f(v, 0.4305f, 0.3416f, 0.1783f, 0.2220f, 0.7067f, 0.07132f, 0.0202f, 0.1296f, 0.9391f);
+        break;
+    case Vship_PRIMARIES_BT470_M:
+        v = mat3f(v, 0.6068f, 0.1735f, 0.2003f, 0.2989f, 0.5866f, 0.1145f, 0.f, 0.06609f, 1.116f);
+        break;
+    default: break;  // INTERNAL: already XYZ
+    }
+    return mat3f(v, 3.2410f, -1.5374f, -0.4986f, -0.9692f, 1.8760f, 0.0416f, 0.0556f, -0.2040f, 1.0570f);
+}
+
+// Linear BT.709 RGB of luma position (X, Y) of one raw image.
+__device__ __forceinline__ float3 ingest_pixel(const RawImage& im, int64_t X, int64_t Y, const ColourParams& cp) {
+    float3 v;
+    v.x = load_norm(im.p[0], im.stride[0], X, Y, cp, false);
+    v.y = chroma_at(im, 1, X, Y, cp);
+    v.z = chroma_at(im, 2, X, Y, cp);
+    if (!cp.skip_yuv) {
+        v = gamma_light(v, cp.matrix);
+        v = transfer(v, cp.trc);
+        v = linear_light(v, cp.matrix);
+    }
+    return primaries_to_709(v, cp.primaries);
+}
+
+}  // namespace vship

@@ -1,0 +1,50 @@
+// Internal interfaces between the C ABI layer (api.cu) and the metric engines.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace vship {
+
+// SSIMULACRA2 engine of one handler (replaces ssimu2::SSIMU2ComputingImplementation,
+// src/ssimu2/main.hpp:80-156).  All device memory is allocated by init.
+struct Ssimu2Api {
+    virtual ~Ssimu2Api() = default;
+    virtual void init(const Vship_Colorspace_t& src, const Vship_Colorspace_t& dis, int device) = 0;
+    // Host planes; blocks until the score is known.
+    virtual double compute(const uint8_t* const s1[3], const uint8_t* const s2[3], const int64_t ls1[3],
+                           const int64_t ls2[3]) = 0;
+    // n pairs already in device memory (3 plane pointers per image); asynchronous on `stream`.
+    virtual void compute_device(int n, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t ls1[3],
+                                const int64_t ls2[3], double* d_scores, float* d_features, cudaStream_t stream) = 0;
+    virtual void last_features(float out[108]) = 0;
+    virtual KernelTimer& timer() = 0;
+    virtual int width() const = 0;
+    virtual int height() const = 0;
+};
+
+// Butteraugli engine of one handler (replaces butter::ButterComputingImplementation,
+// src/butter/main.hpp:183-231).
+struct ButterApi {
+    virtual ~ButterApi() = default;
+    virtual void init(const Vship_Colorspace_t& src, const Vship_Colorspace_t& dis, int qnorm, float intensity,
+                      int device) = 0;
+    // Host planes; dstp (nullable) receives the FP32 distortion map with row stride dststride.
+    virtual void compute(double norms[3], uint8_t* dstp, int64_t dststride, const uint8_t* const s1[3],
+                         const uint8_t* const s2[3], const int64_t ls1[3], const int64_t ls2[3]) = 0;
+    // One pair already in device memory; asynchronous on `stream`.  d_norms receives 3 doubles,
+    // d_distmap (nullable) the map with row stride dststride bytes.
+    virtual void compute_device(double* d_norms, float* d_distmap, int64_t dststride, const uint8_t* const d1[3],
+                                const uint8_t* const d2[3], const int64_t ls1[3], const int64_t ls2[3],
+                                cudaStream_t stream) = 0;
+    virtual KernelTimer& timer() = 0;
+    virtual int width() const = 0;
+    virtual int height() const = 0;
+};
+
+Ssimu2Api* make_ssimu2_engine();
+ButterApi* make_butter_engine();
+
+}  // namespace vship

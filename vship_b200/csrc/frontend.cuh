@@ -1,0 +1,196 @@
+// Host side of the colour front-end: turns a Vship_Colorspace_t into ColourParams and the
+// input geometry, stages host planes into device memory, and provides the optional
+// resize + crop path (Converter::convert, src/gpuColorToLinear/vshipColor.hpp:36-146).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+#include "common.cuh"
+#include "colour.cuh"
+
+namespace vship {
+
+inline int sample_bytes(int s) {
+    switch (s) {
+    case Vship_SampleUINT8: return 1;
+    case Vship_SampleFLOAT: return 4;
+    case Vship_SampleHALF:
+    case Vship_SampleUINT9:
+    case Vship_SampleUINT10:
+    case Vship_SampleUINT12:
+    case Vship_SampleUINT14:
+    case Vship_SampleUINT16: return 2;
+    default: return 0;
+    }
+}
+
+inline int sample_bits(int s) {
+    switch (s) {
+    case Vship_SampleUINT8: return 8;
+    case Vship_SampleUINT9: return 9;
+    case Vship_SampleUINT10: return 10;
+    case Vship_SampleUINT12: return 12;
+    case Vship_SampleUINT14: return 14;
+    case Vship_SampleUINT16: return 16;
+    default: return 1;
+    }
+}
+
+// Geometry of one input clip.
+struct ClipGeometry {
+    int64_t W = 0, H = 0;          // luma plane size as delivered
+    int64_t pw[3] = {0, 0, 0}, ph[3] = {0, 0, 0};
+    int64_t TW = 0, TH = 0;        // size after the optional resize
+    int64_t OW = 0, OH = 0;        // size after crop: the metric's size
+    int crop_top = 0, crop_left = 0;
+    bool resized = false, cropped = false;
+    int bytes = 0;
+    bool generic() const { return resized || cropped; }
+};
+
+inline ClipGeometry make_geometry(const Vship_Colorspace_t& cs) {
+    ClipGeometry g;
+    g.bytes = sample_bytes(cs.sample);
+    if (g.bytes == 0) VSHIP_THROW(Vship_BadErrorType, "unknown Vship_Sample_t value " + std::to_string((int)cs.sample));
+    if (cs.width <= 0 || cs.height <= 0) VSHIP_THROW(Vship_BadErrorType, "width and height must be positive");
+    if (cs.subsampling.subw < 0 || cs.subsampling.subw > 2 || cs.subsampling.subh < 0 || cs.subsampling.subh > 1)
+        VSHIP_THROW(Vship_BadErrorType, "chroma subsampling must satisfy subw in [0,2] and subh in [0,1]");
+    g.W = cs.width;
+    g.H = cs.height;
+    for (int c = 0; c < 3; c++) {
+        g.pw[c] = c ? ((g.W - 1) >> cs.subsampling.subw) + 1 : g.W;
+        g.ph[c] = c ? ((g.H - 1) >> cs.subsampling.subh) + 1 : g.H;
+    }
+    g.TW = cs.target_width == -1 ? g.W : cs.target_width;
+    g.TH = cs.target_height == -1 ? g.H : cs.target_height;
+    if (g.TW <= 0 || g.TH <= 0) VSHIP_THROW(Vship_BadErrorType, "target size must be positive or -1");
+    g.resized = (g.TW != g.W || g.TH != g.H);
+    g.cropped = cs.crop.top != 0 || cs.crop.bottom != 0 || cs.crop.left != 0 || cs.crop.right != 0;
+    g.crop_top = cs.crop.top;
+    g.crop_left = cs.crop.left;
+    g.OW = g.TW - cs.crop.left - cs.crop.right;
+    g.OH = g.TH - cs.crop.top - cs.crop.bottom;
+    if (cs.crop.top < 0 || cs.crop.bottom < 0 || cs.crop.left < 0 || cs.crop.right < 0 || g.OW <= 0 || g.OH <= 0)
+        VSHIP_THROW(Vship_BadErrorType, "crop rectangle leaves no pixels");
+    return g;
+}
+
+inline ColourParams make_colour_params(const Vship_Colorspace_t& cs, const ClipGeometry& g, bool misaligned) {
+    ColourParams cp{};
+    cp.sample = cs.sample;
+    cp.bytes = g.bytes;
+    const int bits = sample_bits(cs.sample);
+    cp.mask = bits >= 16 ? 0xFFFFu : ((1u << bits) - 1u);
+    cp.misaligned = misaligned ? 1 : 0;
+    cp.full_range = cs.range == Vship_RangeFull;
+    cp.full_norm = (float)((1 << bits) - 1);
+    cp.lim_div = bits >= 8 ? (float)(1 << (bits - 8)) : 0.f;
+    cp.yuv_chroma = cs.colorFamily == Vship_ColorYUV;
+    cp.subw = cs.subsampling.subw;
+    cp.subh = cs.subsampling.subh;
+    cp.hcenter = (cs.chromaLocation == Vship_ChromaLoc_Center || cs.chromaLocation == Vship_ChromaLoc_Top);
+    cp.vcenter = (cs.chromaLocation == Vship_ChromaLoc_Center || cs.chromaLocation == Vship_ChromaLoc_Left);
+    cp.matrix = cs.YUVMatrix;
+    cp.trc = cs.transferFunction;
+    cp.primaries = cs.primaries;
+    cp.skip_yuv = (cs.transferFunction == Vship_TRC_Linear && cs.YUVMatrix == Vship_MATRIX_RGB);
+    cp.W = g.W;
+    cp.H = g.H;
+    cp.cw = g.pw[1];
+    cp.ch = g.ph[1];
+    return cp;
+}
+
+// Bytes of one dense device copy of an image (planes back to back, each 256-byte aligned).
+inline int64_t dense_image_bytes(const ClipGeometry& g, int64_t plane_off[3]) {
+    int64_t off = 0;
+    for (int c = 0; c < 3; c++) {
+        plane_off[c] = off;
+        off += round_up(g.pw[c] * g.bytes * g.ph[c], 256);
+    }
+    return off;
+}
+
+// Copies three host planes with arbitrary byte strides into a dense device image.
+inline void stage_host_image(uint8_t* dst, const int64_t plane_off[3], const ClipGeometry& g,
+                             const uint8_t* const src[3], const int64_t line_size[3], cudaStream_t stream) {
+    for (int c = 0; c < 3; c++) {
+        if (src[c] == nullptr) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
+        const int64_t row = g.pw[c] * g.bytes;
+        if (line_size[c] < row) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
+        if (line_size[c] == row) {
+            CUDA_CHECK(cudaMemcpyAsync(dst + plane_off[c], src[c], (size_t)(row * g.ph[c]), cudaMemcpyHostToDevice, stream));
+        } else {
+            CUDA_CHECK(cudaMemcpy2DAsync(dst + plane_off[c], (size_t)row, src[c], (size_t)line_size[c], (size_t)row,
+                                         (size_t)g.ph[c], cudaMemcpyHostToDevice, stream));
+        }
+    }
+}
+
+// ---- generic path: ingest to planar linear RGB, then resize (horizontalResizeTranspose,
+// ---- src/gpuColorToLinear/resize.hpp:26-48), crop by offset.
+
+static __global__ void ingest_linear_kernel(RawImage im, ColourParams cp, float* out, int64_t plane_stride) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cp.W * cp.H) return;
+    const int64_t X = i % cp.W, Y = i / cp.W;
+    const float3 v = ingest_pixel(im, X, Y, cp);
+    out[i] = v.x;
+    out[plane_stride + i] = v.y;
+    out[2 * plane_stride + i] = v.z;
+}
+
+// One pass of the separable resize: rows of length sw resized to rw samples, written
+// transposed (dst is rw x sh).  The source coordinate is formed in float as in the reference.
+static __global__ void resize_transpose_kernel(const float* src, float* dst, int64_t sw, int64_t sh, int64_t rw) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rw * sh) return;
+    const int64_t x = i % rw, y = i / rw;
+    const float approx = (float)x * (float)sw / (float)rw;
+    const int64_t b = (int64_t)approx;
+    const float* row = src + y * sw;
+    const float v1 = row[b];
+    const float v0 = b - 1 >= 0 ? row[b - 1] : v1;
+    const float v2 = b + 1 < sw ? row[b + 1] : v1;
+    const float v3 = b + 2 < sw ? row[b + 2] : v2;
+    dst[x * sh + y] = hermite(v1, (v2 - v0) / 2.f, v2, (v3 - v1) / 2.f, approx - (float)b);
+}
+
+// Linear RGB of the generic path: planes of TW x TH floats (after resize); the metric reads
+// the crop window at offset crop_top * TW + crop_left with pitch TW.
+struct GenericLinear {
+    float* planes = nullptr;   // 3 * TW * TH
+    float* scratch = nullptr;  // W*H*3 (ingest) + TW*H (resize intermediate)
+    int64_t plane_floats = 0;
+
+    void alloc(const ClipGeometry& g) {
+        plane_floats = g.TW * g.TH;
+        planes = device_alloc<float>((size_t)(3 * plane_floats), "resized linear planes");
+        if (g.resized) scratch = device_alloc<float>((size_t)(3 * g.W * g.H + g.TW * g.H), "resize scratch");
+    }
+    void free() {
+        device_free(planes);
+        device_free(scratch);
+        planes = scratch = nullptr;
+    }
+    void run(const RawImage& im, const ColourParams& cp, const ClipGeometry& g, cudaStream_t stream) {
+        const int64_t n = g.W * g.H;
+        float* lin = g.resized ? scratch : planes;
+        const int64_t lin_stride = g.resized ? n : plane_floats;
+        ingest_linear_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, stream>>>(im, cp, lin, lin_stride);
+        CUDA_CHECK(cudaGetLastError());
+        if (!g.resized) return;
+        float* mid = scratch + 3 * n;
+        for (int c = 0; c < 3; c++) {
+            resize_transpose_kernel<<<(unsigned)ceil_div(g.TW * g.H, 256), 256, 0, stream>>>(lin + c * n, mid, g.W, g.H, g.TW);
+            CUDA_CHECK(cudaGetLastError());
+            resize_transpose_kernel<<<(unsigned)ceil_div(g.TH * g.TW, 256), 256, 0, stream>>>(mid, planes + c * plane_floats, g.H, g.TW, g.TH);
+            CUDA_CHECK(cudaGetLastError());
+        }
+    }
+    const float* window() const { return planes; }
+};
+
+}  // namespace vship

@@ -1,0 +1,687 @@
+// SSIMULACRA2 engine for B200 (sm_100a).
+//
+// Per frame pair the reference (src/ssimu2/main.hpp:27-156, score.hpp:380-460) runs about
+// 70 launches: colour conversion, 30 box downsamples, one XYB pass, 11 map kernels with
+// 1-2 tree reductions each, then a blocking copy of 108 floats and the score on the host.
+// This engine runs three kernels for any number of pairs of one handler:
+//
+//   1. ssimu2_front_kernel  raw planes -> linear RGB -> 6-level 2x box pyramid -> positive XYB
+//                           (one 64x64 tile of level 0 per CTA; levels 1-5 of the tile are
+//                           built in shared memory; only planes some map reads are stored)
+//   2. ssimu2_maps_kernel   one launch over a work list of 32x32 output tiles of every
+//                           unpruned (pair, plane, scale): 48x48 halo tiles of both images,
+//                           separable 17-tap renormalised blur of a, b, ab and a^2+b^2 in
+//                           shared memory, SSIM / artifact / detail-loss maps, per-tile sums
+//                           of x and x^4 in FP64
+//   3. ssimu2_final_kernel  per pair: FP64 sum of tile partials, 4th roots, the 108 features
+//                           and the score, computed like the reference's final_score
+//
+// Storage is FP32 end to end: storing levels in FP16 biases the SSIM 1-norms by ~1e-5 per
+// pixel (quantisation noise adds ~2e-8 to each local variance), which moves the score by
+// ~1e-2, ten times the accepted error.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "common.cuh"
+#include "colour.cuh"
+#include "frontend.cuh"
+#include "metric_tables.h"
+#include "engines.h"
+
+namespace vship {
+namespace ssimu2 {
+
+constexpr int kScales = 6;
+
+// Pyramid of one image: level sizes and the float offset of each stored XYB plane.
+struct Pyramid {
+    int w[kScales], h[kScales], pitch[kScales];
+    int64_t off[kScales][3];  // -1 when no map reads the plane
+    int64_t image_floats;
+};
+
+inline bool map_on(int plane, int scale, int map) {
+    return kSsimu2Weights[plane * 36 + scale * 6 + map] > VSHIP_SSIMU2_PRUNE ||
+           kSsimu2Weights[plane * 36 + scale * 6 + 3 + map] > VSHIP_SSIMU2_PRUNE;
+}
+
+inline bool plane_needed(int plane, int scale) {
+    return map_on(plane, scale, 0) || map_on(plane, scale, 1) || map_on(plane, scale, 2);
+}
+
+// 17-tap Gaussian, sigma 1.5, and its prefix sums (src/ssimu2/gaussianblur.hpp:7-18).
+// The normalisation constant cancels in the per-pixel renormalisation.
+__constant__ float c_gauss[17];
+__constant__ float c_gauss_prefix[18];
+__constant__ double c_weights[108] = {VSHIP_SSIMU2_WEIGHT_LIST};
+
+// positive XYB of a linear RGB triple (src/ssimu2/makeXYB.hpp:6-47).
+__device__ __forceinline__ float3 positive_xyb(float3 a) {
+    const float bias = 0.0037930734f;
+    float l = fmaf(0.30f, a.x, fmaf(0.622f, a.y, fmaf(0.078f, a.z, bias)));
+    float m = fmaf(0.23f, a.x, fmaf(0.692f, a.y, fmaf(0.078f, a.z, bias)));
+    float s = fmaf(0.24342269f, a.x, fmaf(0.20476745f, a.y, fmaf(0.55180986f, a.z, bias)));
+    const float absb = -0.1559542025327239f;
+    l = cbrtf(fmaxf(l, 0.f)) + absb;
+    m = cbrtf(fmaxf(m, 0.f)) + absb;
+    s = cbrtf(fmaxf(s, 0.f)) + absb;
+    const float X = 0.5f * (l - m);
+    const float Y = X + m;
+    float3 r;
+    r.z = (float)((double)(s - Y) + 0.55);
+    r.x = (float)((double)(X * 14.0f) + 0.42);
+    r.y = (float)((double)Y + 0.01);
+    return r;
+}
+
+constexpr int kMaxBatch = 64;  // pairs per launch
+
+struct FrontArgs {
+    ColourParams cp[2];      // [0] reference clip, [1] distorted clip
+    const float* lin[2];     // generic path: linear RGB planes of the two clips (crop window)
+    int64_t lin_plane[2];    // floats between planes
+    int64_t lin_pitch[2];    // row pitch of the linear planes
+    float* xyb;              // pyramid base; image i starts at xyb + i * pyr.image_floats
+    Pyramid pyr;
+    RawImage raw[2 * kMaxBatch];  // one per image (images alternate reference / distorted)
+};
+
+// Shared-memory tile of one pyramid level: 3 channels of T x T (+1 pad column).
+template <int T>
+struct LevelTile {
+    float v[3][T][T + 1];
+};
+
+// Builds level L (tile size T) of the CTA's tile from level L-1 held in `src` (tile size
+// 2T), writes its XYB planes, keeps its linear RGB in `dst`.  Downsample order and clamps
+// follow src/ssimu2/downsample.hpp:3-19.
+template <int T>
+__device__ __forceinline__ void build_level(const LevelTile<2 * T>& src, LevelTile<T>& dst, int L,
+                                            const FrontArgs& a, float* img_out) {
+    const int W = a.pyr.w[L], H = a.pyr.h[L], Wp = a.pyr.w[L - 1], Hp = a.pyr.h[L - 1];
+    const int ox = blockIdx.x * T, oy = blockIdx.y * T;
+    for (int i = threadIdx.x; i < T * T; i += blockDim.x) {
+        const int lx = i % T, ly = i / T;
+        const int gx = ox + lx, gy = oy + ly;
+        if (gx >= W || gy >= H) continue;
+        const int x0 = 2 * gx - 2 * ox, y0 = 2 * gy - 2 * oy;
+        const int x1 = min(2 * gx + 1, Wp - 1) - 2 * ox, y1 = min(2 * gy + 1, Hp - 1) - 2 * oy;
+        float3 d;
+        float* dp = &d.x;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            float t = src.v[c][y0][x0];
+            t += src.v[c][y1][x0];
+            t += src.v[c][y0][x1];
+            t += src.v[c][y1][x1];
+            t *= 0.25f;
+            dp[c] = t;
+            dst.v[c][ly][lx] = t;
+        }
+        const float3 q = positive_xyb(d);
+        const float qv[3] = {q.x, q.y, q.z};
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+            if (a.pyr.off[L][p] >= 0) img_out[a.pyr.off[L][p] + (int64_t)gy * a.pyr.pitch[L] + gx] = qv[p];
+    }
+}
+
+template <bool FromLinear>
+__global__ void __launch_bounds__(256) ssimu2_front_kernel(const __grid_constant__ FrontArgs a) {
+    __shared__ LevelTile<32> t1;
+    __shared__ LevelTile<16> t2;
+    __shared__ LevelTile<8> t3;
+    __shared__ LevelTile<4> t4;
+    __shared__ LevelTile<2> t5;
+    const int img = blockIdx.z;
+    const int clip = img & 1;
+    const ColourParams& cp = a.cp[clip];
+    float* out = a.xyb + (int64_t)img * a.pyr.image_floats;
+    const int W0 = a.pyr.w[0], H0 = a.pyr.h[0], W1 = a.pyr.w[1], H1 = a.pyr.h[1];
+    const int pitch0 = a.pyr.pitch[0];
+    float* y0plane = out + a.pyr.off[0][1];
+    const RawImage& im = a.raw[img];
+
+    auto pixel = [&](int X, int Y) -> float3 {
+        if (FromLinear) {
+            const float* base = a.lin[clip] + (int64_t)Y * a.lin_pitch[clip] + X;
+            return make_float3(base[0], base[a.lin_plane[clip]], base[2 * a.lin_plane[clip]]);
+        } else {
+            return ingest_pixel(im, X, Y, cp);
+        }
+    };
+
+    // Level 0 -> level 1: one 2x2 quad of level 0 per work item.
+    for (int q = threadIdx.x; q < 32 * 32; q += blockDim.x) {
+        const int qx = q & 31, qy = q >> 5;
+        const int gx = blockIdx.x * 32 + qx, gy = blockIdx.y * 32 + qy;
+        if (gx >= W1 || gy >= H1) continue;
+        const int X0 = 2 * gx, Y0 = 2 * gy;
+        const int X1 = min(X0 + 1, W0 - 1), Y1 = min(Y0 + 1, H0 - 1);
+        const float3 p00 = pixel(X0, Y0);
+        const float3 p01 = (X1 != X0) ? pixel(X1, Y0) : p00;
+        const float3 p10 = (Y1 != Y0) ? pixel(X0, Y1) : p00;
+        const float3 p11 = (Y1 != Y0) ? ((X1 != X0) ? pixel(X1, Y1) : p10) : p01;
+        // Level-0 XYB: only the Y plane has unpruned maps at full resolution.
+        const float y00 = positive_xyb(p00).y;
+        if (X1 != X0) {
+            *reinterpret_cast<float2*>(y0plane + (int64_t)Y0 * pitch0 + X0) = make_float2(y00, positive_xyb(p01).y);
+            if (Y1 != Y0)
+                *reinterpret_cast<float2*>(y0plane + (int64_t)Y1 * pitch0 + X0) =
+                    make_float2(positive_xyb(p10).y, positive_xyb(p11).y);
+        } else {
+            y0plane[(int64_t)Y0 * pitch0 + X0] = y00;
+            if (Y1 != Y0) y0plane[(int64_t)Y1 * pitch0 + X0] = positive_xyb(p10).y;
+        }
+        float3 d;
+        d.x = p00.x; d.x += p10.x; d.x += p01.x; d.x += p11.x; d.x *= 0.25f;
+        d.y = p00.y; d.y += p10.y; d.y += p01.y; d.y += p11.y; d.y *= 0.25f;
+        d.z = p00.z; d.z += p10.z; d.z += p01.z; d.z += p11.z; d.z *= 0.25f;
+        t1.v[0][qy][qx] = d.x;
+        t1.v[1][qy][qx] = d.y;
+        t1.v[2][qy][qx] = d.z;
+        const float3 x1 = positive_xyb(d);
+        const float xv[3] = {x1.x, x1.y, x1.z};
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+            if (a.pyr.off[1][p] >= 0) out[a.pyr.off[1][p] + (int64_t)gy * a.pyr.pitch[1] + gx] = xv[p];
+    }
+    __syncthreads();
+    build_level<16>(t1, t2, 2, a, out);
+    __syncthreads();
+    build_level<8>(t2, t3, 3, a, out);
+    __syncthreads();
+    build_level<4>(t3, t4, 4, a, out);
+    __syncthreads();
+    build_level<2>(t4, t5, 5, a, out);
+}
+
+// One unpruned (pair, plane, scale) of the map work list.
+struct MapSeg {
+    const float* a;       // reference XYB plane
+    const float* b;       // distorted XYB plane
+    int w, h, pitch;
+    int tiles_x;
+    int tile_begin;       // first global tile index of this segment
+    int ntiles;
+    int slot;             // plane * 36 + scale * 6
+    int on;               // bit k set: map k (ssim, artifact, detail-loss) is unpruned
+};
+
+constexpr int kTile = 32;
+constexpr int kHalo = 8;
+constexpr int kIn = kTile + 2 * kHalo;  // 48
+
+__device__ __forceinline__ float blur_norm(int pos, int n) {
+    // Sum of the taps of a 17-tap window centred on pos that fall inside [0, n).
+    const int beg = max(0, kHalo - pos);
+    const int end = min(17, n + kHalo - pos);
+    return c_gauss_prefix[end] - c_gauss_prefix[beg];
+}
+
+__global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restrict__ segs, int nseg,
+                                                          double* __restrict__ partials) {
+    __shared__ float sa[kIn][kIn + 1];
+    __shared__ float sb[kIn][kIn + 1];
+    __shared__ float sh[4][kIn][kTile + 1];
+    __shared__ double red[8][6];
+    __shared__ int s_seg;
+
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nseg - 1;
+        const int t = blockIdx.x;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segs[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
+        }
+        s_seg = lo;
+    }
+    __syncthreads();
+    const MapSeg sg = segs[s_seg];
+    const int local = blockIdx.x - sg.tile_begin;
+    const int X0 = (local % sg.tiles_x) * kTile, Y0 = (local / sg.tiles_x) * kTile;
+    const int tid = threadIdx.x;
+
+    // Halo tiles of both images; zero outside the plane (src/ssimu2/gaussianblur.hpp:24-36).
+    for (int i = tid; i < kIn * kIn; i += 256) {
+        const int r = i / kIn, c = i % kIn;
+        const int gx = X0 - kHalo + c, gy = Y0 - kHalo + r;
+        float va = 0.f, vb = 0.f;
+        if (gx >= 0 && gx < sg.w && gy >= 0 && gy < sg.h) {
+            const int64_t o = (int64_t)gy * sg.pitch + gx;
+            va = __ldg(sg.a + o);
+            vb = __ldg(sg.b + o);
+        }
+        sa[r][c] = va;
+        sb[r][c] = vb;
+    }
+    __syncthreads();
+
+    // Horizontal pass: 48 rows x 32 columns of the four moment inputs, two adjacent
+    // output columns per work item, divided by the in-bounds tap sum of their column.
+    for (int u = tid; u < kIn * (kTile / 2); u += 256) {
+        const int r = u >> 4, c0 = (u & 15) * 2;
+        float av[18], bv[18], pv[18], qv[18];
+#pragma unroll
+        for (int j = 0; j < 18; j++) {
+            av[j] = sa[r][c0 + j];
+            bv[j] = sb[r][c0 + j];
+            pv[j] = __fmul_rn(av[j], bv[j]);
+            qv[j] = __fadd_rn(__fmul_rn(av[j], av[j]), __fmul_rn(bv[j], bv[j]));
+        }
+        float acc[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+        for (int j = 0; j < 17; j++) {
+            const float g = c_gauss[j];
+#pragma unroll
+            for (int o = 0; o < 2; o++) {
+                acc[0][o] = fmaf(g, av[j + o], acc[0][o]);
+                acc[1][o] = fmaf(g, bv[j + o], acc[1][o]);
+                acc[2][o] = fmaf(g, pv[j + o], acc[2][o]);
+                acc[3][o] = fmaf(g, qv[j + o], acc[3][o]);
+            }
+        }
+#pragma unroll
+        for (int o = 0; o < 2; o++) {
+            const float tot = blur_norm(X0 + c0 + o, sg.w);
+#pragma unroll
+            for (int q = 0; q < 4; q++) sh[q][r][c0 + o] = acc[q][o] / tot;
+        }
+    }
+    __syncthreads();
+
+    // Vertical pass: each thread 4 consecutive output rows of one column.
+    const int c = tid & 31, r0 = (tid >> 5) * 4;
+    float mo[4][4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        float col[20];
+#pragma unroll
+        for (int j = 0; j < 20; j++) col[j] = sh[q][r0 + j][c];
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+            float acc = 0.f;
+#pragma unroll
+            for (int j = 0; j < 17; j++) acc = fmaf(c_gauss[j], col[o + j], acc);
+            mo[q][o] = acc;
+        }
+    }
+    float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const int gx = X0 + c;
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+        const int gy = Y0 + r0 + o;
+        if (gx >= sg.w || gy >= sg.h) continue;
+        const float tot = blur_norm(gy, sg.h);
+        const float m1 = mo[0][o] / tot, m2 = mo[1][o] / tot, s12 = mo[2][o] / tot, ssq = mo[3][o] / tot;
+        // SSIM map (src/ssimu2/score.hpp:266-274) with a^2+b^2 blurred directly; rounding is
+        // explicit so that identical inputs give exactly 0.
+        const float mu = __fmul_rn(m1, m2);
+        const float m11 = __fmul_rn(m1, m1), m22 = __fmul_rn(m2, m2);
+        const float md = __fsub_rn(m1, m2);
+        const float num_m = __fsub_rn(1.0f, __fmul_rn(md, md));
+        const float num_s = __fadd_rn(__fmul_rn(2.0f, __fsub_rn(s12, mu)), 0.0009f);
+        const float den_s = __fadd_rn(__fsub_rn(ssq, __fadd_rn(m11, m22)), 0.0009f);
+        const float ssim = fmaxf(1.0f - (num_m * num_s) / den_s, 0.0f);
+        // Artifact and detail-loss maps (score.hpp:276-281).
+        const float ca = sa[r0 + o + kHalo][c + kHalo], cb = sb[r0 + o + kHalo][c + kHalo];
+        const float v1 = (fabsf(cb - m2) + 1.0f) / (fabsf(ca - m1) + 1.0f) - 1.0f;
+        const float art = fmaxf(v1, 0.0f), det = fmaxf(-v1, 0.0f);
+        const float s2 = ssim * ssim, a2 = art * art, d2 = det * det;
+        sum[0] += ssim; sum[1] += art; sum[2] += det;
+        sum[3] += s2 * s2; sum[4] += a2 * a2; sum[5] += d2 * d2;
+    }
+    // FP64 tree reduction of the tile.
+    double dsum[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        double v = (double)sum[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        dsum[k] = v;
+    }
+    const int warp = tid >> 5, lane = tid & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) red[warp][k] = dsum[k];
+    }
+    __syncthreads();
+    if (tid < 6) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; w++) v += red[w][tid];
+        partials[(int64_t)blockIdx.x * 6 + tid] = v;
+    }
+}
+
+// Per pair: FP64 totals of the tile partials, the 108 features, and the score exactly as
+// final_score computes it (src/ssimu2/score.hpp:442-460: float fmaf accumulation, float
+// result).
+__global__ void __launch_bounds__(256) ssimu2_final_kernel(const MapSeg* __restrict__ segs, int segs_per_pair,
+                                                           const double* __restrict__ partials,
+                                                           double* __restrict__ scores, float* __restrict__ features) {
+    __shared__ double red[8][6];
+    __shared__ float feat[108];
+    const int pair = blockIdx.x, tid = threadIdx.x;
+    for (int i = tid; i < 108; i += 256) feat[i] = 0.f;
+    __syncthreads();
+    for (int s = 0; s < segs_per_pair; s++) {
+        const MapSeg sg = segs[pair * segs_per_pair + s];
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int t = tid; t < sg.ntiles; t += 256) {
+            const double* p = partials + (int64_t)(sg.tile_begin + t) * 6;
+#pragma unroll
+            for (int k = 0; k < 6; k++) acc[k] += p[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], off);
+        }
+        if ((tid & 31) == 0) {
+#pragma unroll
+            for (int k = 0; k < 6; k++) red[tid >> 5][k] = acc[k];
+        }
+        __syncthreads();
+        if (tid < 3) {
+            const double n = (double)sg.w * (double)sg.h;
+            double s1 = 0.0, s4 = 0.0;
+            for (int w = 0; w < 8; w++) { s1 += red[w][tid]; s4 += red[w][3 + tid]; }
+            const bool on = (sg.on >> tid) & 1;
+            feat[sg.slot + tid] = on ? (float)(s1 / n) : 0.f;
+            feat[sg.slot + 3 + tid] = on ? (float)sqrt(sqrt(s4 / n)) : 0.f;
+        }
+        __syncthreads();
+    }
+    if (features)
+        for (int i = tid; i < 108; i += 256) features[(int64_t)pair * 108 + i] = feat[i];
+    if (tid == 0) {
+        double s = 0.0;
+        for (int i = 0; i < 108; i++) s = (double)fmaf((float)c_weights[i], feat[i], (float)s);
+        s *= VSHIP_SSIMU2_SCALE;
+        s = (VSHIP_SSIMU2_C3 * s * s) * s + VSHIP_SSIMU2_C1 * s - VSHIP_SSIMU2_C2 * s * s;
+        s = s > 0.0 ? pow(s, VSHIP_SSIMU2_EXP) * -10.0 + 100.0 : 100.0;
+        scores[pair] = (double)(float)s;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Engine
+// ------------------------------------------------------------------------------------------
+
+static void upload_gauss_constants() {
+    float g[17], pre[18];
+    pre[0] = 0.f;
+    for (int i = 0; i < 17; i++) {
+        g[i] = (float)std::exp(-(double)((8 - i) * (8 - i)) / (2.0 * 1.5 * 1.5));
+        pre[i + 1] = pre[i] + g[i];
+    }
+    CUDA_CHECK(cudaMemcpyToSymbol(c_gauss, g, sizeof(g)));
+    CUDA_CHECK(cudaMemcpyToSymbol(c_gauss_prefix, pre, sizeof(pre)));
+}
+
+class Engine final : public Ssimu2Api {
+public:
+    ~Engine() override { release(); }
+
+    void init(const Vship_Colorspace_t& src, const Vship_Colorspace_t& dis, int device) override {
+        device_ = device;
+        cs_[0] = src;
+        cs_[1] = dis;
+        geo_[0] = make_geometry(src);
+        geo_[1] = make_geometry(dis);
+        if (geo_[0].OW != geo_[1].OW || geo_[0].OH != geo_[1].OH)
+            VSHIP_THROW(Vship_DifferingInputType, "");
+        width_ = (int)geo_[0].OW;
+        height_ = (int)geo_[0].OH;
+        for (int c = 0; c < 2; c++) cp_[c] = make_colour_params(cs_[c], geo_[c], false);
+        generic_ = geo_[0].generic() || geo_[1].generic();
+        build_pyramid();
+        CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        upload_gauss_constants();
+        for (int c = 0; c < 2; c++) {
+            staged_bytes_[c] = dense_image_bytes(geo_[c], staged_off_[c]);
+            staged_[c] = device_alloc<uint8_t>((size_t)staged_bytes_[c], "input staging");
+            if (generic_) lin_[c].alloc(geo_[c]);
+        }
+        score_host_ = pinned_alloc<double>(1, "score");
+        ensure_capacity(1);
+    }
+
+    double compute(const uint8_t* const s1[3], const uint8_t* const s2[3], const int64_t ls1[3], const int64_t ls2[3]) override {
+        stage_host_image(staged_[0], staged_off_[0], geo_[0], s1, ls1, stream_);
+        stage_host_image(staged_[1], staged_off_[1], geo_[1], s2, ls2, stream_);
+        RawImage raw[2];
+        for (int c = 0; c < 2; c++)
+            for (int p = 0; p < 3; p++) {
+                raw[c].p[p] = staged_[c] + staged_off_[c][p];
+                raw[c].stride[p] = geo_[c].pw[p] * geo_[c].bytes;
+            }
+        run_pairs(1, raw, cp_, stream_, scores_d_, features_d_);
+        CUDA_CHECK(cudaMemcpyAsync(score_host_, scores_d_, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CUDA_CHECK(cudaMemcpyAsync(last_features_, features_d_, sizeof(float) * 108, cudaMemcpyDeviceToHost, stream_));
+        CUDA_CHECK(cudaStreamSynchronize(stream_));
+        return *score_host_;
+    }
+
+    void compute_device(int n, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t ls1[3],
+                        const int64_t ls2[3], double* d_scores, float* d_features, cudaStream_t stream) override {
+        if (n <= 0) return;
+        if (generic_ && n > 1) {
+            for (int i = 0; i < n; i++)
+                compute_device(1, d1 + 3 * i, d2 + 3 * i, ls1, ls2, d_scores ? d_scores + i : nullptr,
+                               d_features ? d_features + (int64_t)i * 108 : nullptr, stream);
+            return;
+        }
+        ColourParams cp[2] = {cp_[0], cp_[1]};
+        for (int c = 0; c < 2; c++) {
+            const int64_t* ls = c ? ls2 : ls1;
+            for (int p = 0; p < 3; p++) {
+                if (ls[p] < geo_[c].pw[p] * geo_[c].bytes) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
+                if (ls[p] % geo_[c].bytes) cp[c].misaligned = 1;
+            }
+        }
+        cudaStream_t st = stream ? stream : stream_;
+        std::vector<RawImage> raw(2 * kMaxBatch);
+        int done = 0;
+        while (done < n) {
+            const int chunk = std::min(n - done, kMaxBatch);
+            ensure_capacity(chunk);
+            for (int i = 0; i < chunk; i++)
+                for (int c = 0; c < 2; c++) {
+                    const uint8_t* const* src = c ? d2 : d1;
+                    const int64_t* ls = c ? ls2 : ls1;
+                    for (int p = 0; p < 3; p++) {
+                        if (src[3 * (done + i) + p] == nullptr) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
+                        raw[2 * i + c].p[p] = src[3 * (done + i) + p];
+                        raw[2 * i + c].stride[p] = ls[p];
+                    }
+                }
+            run_pairs(chunk, raw.data(), cp, st, d_scores ? d_scores + done : scores_d_,
+                      d_features ? d_features + (int64_t)done * 108 : features_d_);
+            done += chunk;
+        }
+    }
+
+    void last_features(float out[108]) override { std::memcpy(out, last_features_, sizeof(last_features_)); }
+    KernelTimer& timer() override { return timer_; }
+    int width() const override { return width_; }
+    int height() const override { return height_; }
+
+private:
+    void build_pyramid() {
+        int w = width_, h = height_;
+        int64_t off = 0;
+        for (int s = 0; s < kScales; s++) {
+            pyr_.w[s] = w;
+            pyr_.h[s] = h;
+            pyr_.pitch[s] = (int)round_up(w, 8);
+            for (int p = 0; p < 3; p++) {
+                // Level 0 is only read through its Y plane; the front kernel writes Y there
+                // unconditionally, so Y0 stays allocated whatever the pruning.
+                const bool keep = plane_needed(p, s) || (s == 0 && p == 1);
+                if (keep) {
+                    pyr_.off[s][p] = off;
+                    off += round_up((int64_t)pyr_.pitch[s] * h, 64);
+                } else {
+                    pyr_.off[s][p] = -1;
+                }
+            }
+            w = (w - 1) / 2 + 1;
+            h = (h - 1) / 2 + 1;
+        }
+        pyr_.image_floats = round_up(off, 64);
+        tiles_per_pair_ = 0;
+        segs_per_pair_ = 0;
+        for (int s = 0; s < kScales; s++)
+            for (int p = 0; p < 3; p++)
+                if (plane_needed(p, s)) {
+                    tiles_per_pair_ += (int)(ceil_div(pyr_.w[s], kTile) * ceil_div(pyr_.h[s], kTile));
+                    segs_per_pair_++;
+                }
+    }
+
+    // Work list of the map kernel for `npairs` pairs stored at the start of xyb_.
+    std::vector<MapSeg> build_segments(int npairs) const {
+        std::vector<MapSeg> segs;
+        int tile = 0;
+        for (int pr = 0; pr < npairs; pr++) {
+            for (int s = 0; s < kScales; s++) {
+                for (int p = 0; p < 3; p++) {
+                    int on = 0;
+                    for (int m = 0; m < 3; m++) on |= (map_on(p, s, m) ? 1 : 0) << m;
+                    if (!on) continue;
+                    MapSeg g{};
+                    g.a = xyb_ + (int64_t)(2 * pr) * pyr_.image_floats + pyr_.off[s][p];
+                    g.b = xyb_ + (int64_t)(2 * pr + 1) * pyr_.image_floats + pyr_.off[s][p];
+                    g.w = pyr_.w[s];
+                    g.h = pyr_.h[s];
+                    g.pitch = pyr_.pitch[s];
+                    g.tiles_x = (int)ceil_div(g.w, kTile);
+                    g.ntiles = g.tiles_x * (int)ceil_div(g.h, kTile);
+                    g.tile_begin = tile;
+                    g.slot = p * 36 + s * 6;
+                    g.on = on;
+                    tile += g.ntiles;
+                    segs.push_back(g);
+                }
+            }
+        }
+        return segs;
+    }
+
+    // Grows the batch buffers and rebuilds the work list for kMaxBatch pairs.  The work list
+    // of the first n pairs is a prefix of it, so every batch size shares one table.
+    void ensure_capacity(int npairs) {
+        if (npairs <= cap_) return;
+        const int ncap = npairs <= 1 ? 1 : kMaxBatch;
+        CUDA_CHECK(cudaStreamSynchronize(stream_));
+        device_free(xyb_);
+        device_free(partials_);
+        device_free(segs_d_);
+        device_free(scores_d_);
+        device_free(features_d_);
+        xyb_ = nullptr; partials_ = nullptr; segs_d_ = nullptr; scores_d_ = nullptr; features_d_ = nullptr;
+        xyb_ = device_alloc<float>((size_t)(2 * ncap * pyr_.image_floats), "XYB pyramid");
+        partials_ = device_alloc<double>((size_t)tiles_per_pair_ * 6 * ncap, "tile partials");
+        segs_d_ = device_alloc<MapSeg>((size_t)segs_per_pair_ * ncap, "map work list");
+        scores_d_ = device_alloc<double>((size_t)ncap, "scores");
+        features_d_ = device_alloc<float>((size_t)108 * ncap, "features");
+        const std::vector<MapSeg> segs = build_segments(ncap);
+        CUDA_CHECK(cudaMemcpy(segs_d_, segs.data(), segs.size() * sizeof(MapSeg), cudaMemcpyHostToDevice));
+        cap_ = ncap;
+    }
+
+    void run_pairs(int npairs, const RawImage* raw, const ColourParams cp[2], cudaStream_t st,
+                   double* scores_d, float* features_d) {
+        const int nimg = 2 * npairs;
+        FrontArgs* fa = &front_args_;
+        fa->cp[0] = cp[0];
+        fa->cp[1] = cp[1];
+        fa->xyb = xyb_;
+        fa->pyr = pyr_;
+        for (int i = 0; i < nimg; i++) fa->raw[i] = raw[i];
+        const dim3 fgrid((unsigned)ceil_div(pyr_.w[1], 32), (unsigned)ceil_div(pyr_.h[1], 32), (unsigned)nimg);
+        if (!generic_) {
+            const int t = timer_.begin(0, "ssimu2_front", st);
+            ssimu2_front_kernel<false><<<fgrid, 256, 0, st>>>(*fa);
+            CUDA_CHECK(cudaGetLastError());
+            timer_.end(t, st);
+        } else {
+            // Resize/crop path (one pair): planar linear RGB first, then the pyramid reads the
+            // crop window of each clip.
+            for (int c = 0; c < 2; c++) {
+                lin_[c].run(raw[c], cp[c], geo_[c], st);
+                fa->lin[c] = lin_[c].planes + (int64_t)geo_[c].crop_top * geo_[c].TW + geo_[c].crop_left;
+                fa->lin_plane[c] = geo_[c].TW * geo_[c].TH;
+                fa->lin_pitch[c] = geo_[c].TW;
+            }
+            ssimu2_front_kernel<true><<<fgrid, 256, 0, st>>>(*fa);
+            CUDA_CHECK(cudaGetLastError());
+        }
+        const int ntiles = tiles_per_pair_ * npairs;
+        const int t1 = timer_.begin(1, "ssimu2_maps", st);
+        ssimu2_maps_kernel<<<(unsigned)ntiles, 256, 0, st>>>(segs_d_, segs_per_pair_ * npairs, partials_);
+        CUDA_CHECK(cudaGetLastError());
+        timer_.end(t1, st);
+        const int t2 = timer_.begin(2, "ssimu2_final", st);
+        ssimu2_final_kernel<<<(unsigned)npairs, 256, 0, st>>>(segs_d_, segs_per_pair_, partials_, scores_d, features_d);
+        CUDA_CHECK(cudaGetLastError());
+        timer_.end(t2, st);
+    }
+
+    void release() {
+        if (stream_) (void)cudaStreamSynchronize(stream_);
+        timer_.destroy();
+        for (int c = 0; c < 2; c++) {
+            device_free(staged_[c]);
+            staged_[c] = nullptr;
+            lin_[c].free();
+        }
+        device_free(xyb_);
+        device_free(partials_);
+        device_free(segs_d_);
+        device_free(scores_d_);
+        device_free(features_d_);
+        pinned_free(score_host_);
+        xyb_ = nullptr; partials_ = nullptr; segs_d_ = nullptr; scores_d_ = nullptr; features_d_ = nullptr;
+        score_host_ = nullptr;
+        if (stream_) {
+            (void)cudaStreamDestroy(stream_);
+            stream_ = nullptr;
+        }
+    }
+
+    int device_ = 0;
+    Vship_Colorspace_t cs_[2];
+    ClipGeometry geo_[2];
+    ColourParams cp_[2];
+    bool generic_ = false;
+    Pyramid pyr_{};
+    int tiles_per_pair_ = 0, segs_per_pair_ = 0;
+    int width_ = 0, height_ = 0;
+    cudaStream_t stream_ = nullptr;
+    uint8_t* staged_[2] = {nullptr, nullptr};
+    int64_t staged_off_[2][3] = {};
+    int64_t staged_bytes_[2] = {0, 0};
+    GenericLinear lin_[2];
+    float* xyb_ = nullptr;
+    double* partials_ = nullptr;
+    MapSeg* segs_d_ = nullptr;
+    double* scores_d_ = nullptr;
+    float* features_d_ = nullptr;
+    double* score_host_ = nullptr;
+    float last_features_[108] = {};
+    int cap_ = 0;
+    FrontArgs front_args_{};
+    KernelTimer timer_;
+};
+
+}  // namespace ssimu2
+
+Ssimu2Api* make_ssimu2_engine() { return new ssimu2::Engine(); }
+
+}  // namespace vship
