@@ -17,8 +17,8 @@ extern "C" {
 
 /* Scores n frame pairs whose planes are already in device memory of the handler's GPU.
  * srcp1 and srcp2 are host arrays of 3*n device plane pointers (pair i uses entries 3i..3i+2),
- * with the same byte strides for every pair.  Work is queued on `stream` (a cudaStream_t, or
- * NULL for the handler's own stream) and the call returns without waiting: d_scores (device,
+ * with the same byte strides for every pair.  Work is queued on `stream` (a cudaStream_t;
+ * NULL is the CUDA legacy default stream) and the call returns without waiting: d_scores (device,
  * n doubles) and d_features (device, n*108 floats, may be NULL) are valid once the stream has
  * reached this point.  Up to 64 pairs run in one launch of each kernel. */
 EXPORTPREPROCESS Vship_Exception VshipExt_ComputeSSIMU2Device(Vship_SSIMU2Handler handler, int n, double* d_scores,

@@ -166,20 +166,48 @@ def _golden():
 
 
 def test_oracle_matches_reference_golden_ssimu2(oracle_lib):
+    """Pin of the SSIMULACRA2 restatement against the reference's own outputs.
+
+    The reference evaluates the SSIM map in FP32 as 1 - num/den with variances formed as
+    blur((a+b)^2) - 2 blur(ab) - mu^2 (src/ssimu2/score.hpp:232-274); in smooth regions that
+    cancels ~1e-4 of rounding noise into a map whose values are ~1e-4, and max(., 0) turns the
+    noise into a bias.  Its scores therefore drift from the exact metric by ~1e-3 on frames of
+    60k+ pixels (2e-3 at 1080p) and by up to ~1 on frames of a few pixels (on identical
+    720x480 content it returns 99.89, not 100).  The pin is taken where that drift is below
+    the metric's resolution; the pixel counts and tolerance are stated here."""
     from tests.golden.cases import build_case
     data = _golden()
     checked = 0
     for case in data["cases"]:
-        if case["metric"] != "ssimu2" or case["w"] * case["h"] > 2_100_000:
+        if case["metric"] != "ssimu2" or case.get("identical") or not (60_000 <= case["w"] * case["h"] <= 2_100_000):
             continue
         (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
         q, d, _ = oracle_lib.ssimu2(oracle_lib.convert(p1, ls1, cs1), oracle_lib.convert(p2, ls2, cs2))
-        assert abs(q - case["score"]) <= 1e-3, (case["name"], q, case["score"])
+        assert abs(d - case["score"]) <= 2e-3, (case["name"], d, case["score"])
         checked += 1
-    assert checked >= 5
+    assert checked >= 4
+
+
+def test_reference_fp32_drift_shrinks_with_size(oracle_lib):
+    """The reference/FP64 gap is rounding noise, not an algorithm difference: it is largest
+    on a few pixels and small at full HD for every colourspace of the golden set."""
+    from tests.golden.cases import build_case
+    data = _golden()
+    gaps = {}
+    for case in data["cases"]:
+        if case["metric"] != "ssimu2" or case.get("identical") or case["w"] * case["h"] > 2_100_000:
+            continue
+        (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
+        _, d, _ = oracle_lib.ssimu2(oracle_lib.convert(p1, ls1, cs1), oracle_lib.convert(p2, ls2, cs2))
+        gaps[case["name"]] = abs(d - case["score"])
+    assert gaps["s_rgb8_1920x1080"] < gaps["s_rgb8_64x48"] < gaps["s_rgb8_2x3"]
+    assert max(v for k, v in gaps.items() if "1920" in k or "1921" in k) <= 2e-3
+    assert max(gaps.values()) < 1.0
 
 
 def test_oracle_matches_reference_golden_butteraugli(oracle_lib):
+    """Butteraugli has no such cancellation: the restatement matches the reference's norms
+    to 1e-5 relative and its distortion map samples to 1e-4."""
     from tests.golden.cases import build_case
     data = _golden()
     checked = 0
@@ -191,11 +219,9 @@ def test_oracle_matches_reference_golden_butteraugli(oracle_lib):
                                              case["intensity"], case["qnorm"])
         ref = case["norms"]
         for k in range(3):
-            assert abs(norms[k] - ref[k]) <= 1e-4 * max(abs(ref[k]), 1e-6), (case["name"], k, norms, ref)
-        if "distmap_sample" in case:
-            idx = np.array(case["distmap_sample"]["index"])
-            val = np.array(case["distmap_sample"]["value"])
-            got = dmap.reshape(-1)[idx]
-            np.testing.assert_allclose(got, val, rtol=2e-4, atol=2e-6)
+            assert abs(norms[k] - ref[k]) <= 1e-5 * max(abs(ref[k]), 1e-6), (case["name"], k, norms, ref)
+        idx = np.array(case["distmap_sample"]["index"])
+        val = np.array(case["distmap_sample"]["value"])
+        np.testing.assert_allclose(dmap.reshape(-1)[idx], val, rtol=1e-4, atol=1e-6)
         checked += 1
-    assert checked >= 3
+    assert checked >= 5

@@ -1,7 +1,7 @@
 """GPU parity of the SSIMULACRA2 path through the C ABI against the FP64 oracle.
 
 Tolerance: |dSSIMU2| <= 1e-3 against FP64 (the accuracy bar of the engine); features within
-1e-4 relative.  Identical inputs must give exactly 100, as the reference's identity test
+2e-4 relative (+1e-6 absolute).  Identical inputs must give exactly 100, as the reference's identity test
 requires (test/libvshipTestIdentity.cpp:357-384).
 """
 import numpy as np
@@ -31,7 +31,7 @@ def test_cases_match_oracle(gpu, oracle_lib, case):
         assert got == 100.0
         return
     assert abs(got - d) <= SCORE_TOL, (got, d)
-    np.testing.assert_allclose(feats, f, rtol=1e-4, atol=2e-6)
+    np.testing.assert_allclose(feats, f, rtol=2e-4, atol=1e-6)
 
 
 @pytest.mark.parametrize("fmt,w,h", [("rgb8", 64, 64), ("yuv420p10", 130, 98), ("rgb8", 1920, 1080)])

@@ -54,7 +54,9 @@ def _declare(L):
     L.Vship_ComputeButteraugli.argtypes = [HB, c.POINTER(abi.ButteraugliScore), c.c_void_p, c.c_int64, u8pp, u8pp, i64p, i64p]
     L.Vship_ButteraugliGetDetailedLastError.argtypes = [HB, c.c_char_p, c.c_int]
     L.Vship_ButteraugliGetDetailedLastError.restype = c.c_int
-    # extensions
+    # extensions (absent from the reference library)
+    if not hasattr(L, "VshipExt_ComputeSSIMU2Device"):
+        return L
     vpp = c.POINTER(c.c_void_p)
     L.VshipExt_ComputeSSIMU2Device.argtypes = [H2, c.c_int, c.c_void_p, c.c_void_p, vpp, vpp, i64p, i64p, c.c_void_p]
     L.VshipExt_SSIMU2LastFeatures.argtypes = [H2, c.POINTER(c.c_float)]

@@ -669,6 +669,7 @@ public:
         for (int c = 0; c < 2; c++) cp_[c] = make_colour_params(cs_[c], geo_[c], false);
         generic_ = geo_[0].generic() || geo_[1].generic();
         CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        CUDA_CHECK(cudaEventCreateWithFlags(&last_done_, cudaEventDisableTiming));
         upload_constants();
         for (int c = 0; c < 2; c++) {
             staged_bytes_[c] = dense_image_bytes(geo_[c], staged_off_[c]);
@@ -688,6 +689,7 @@ public:
 
     void compute(double norms[3], uint8_t* dstp, int64_t dststride, const uint8_t* const s1[3], const uint8_t* const s2[3],
                  const int64_t ls1[3], const int64_t ls2[3]) override {
+        CUDA_CHECK(cudaStreamWaitEvent(stream_, last_done_, 0));
         stage_host_image(staged_[0], staged_off_[0], geo_[0], s1, ls1, stream_);
         stage_host_image(staged_[1], staged_off_[1], geo_[1], s2, ls2, stream_);
         RawImage raw[2];
@@ -707,6 +709,7 @@ public:
         if (dstp)
             CUDA_CHECK(cudaMemcpy2DAsync(dstp, (size_t)dststride, distmap_d_, (size_t)w_ * 4, (size_t)w_ * 4, (size_t)h_,
                                          cudaMemcpyDeviceToHost, stream_));
+        CUDA_CHECK(cudaEventRecord(last_done_, stream_));
         CUDA_CHECK(cudaStreamSynchronize(stream_));
         for (int k = 0; k < 3; k++) norms[k] = norms_host_[k];
     }
@@ -728,7 +731,9 @@ public:
         }
         if (d_distmap && (dststride % 4 || dststride < (int64_t)w_ * 4))
             VSHIP_THROW(Vship_BadPointer, "distmap stride must be a multiple of 4 bytes and at least width * 4");
-        run(raw, cp, stream ? stream : stream_, d_norms, d_distmap, dststride / 4);
+        CUDA_CHECK(cudaStreamWaitEvent(stream, last_done_, 0));
+        run(raw, cp, stream, d_norms, d_distmap, dststride / 4);  // NULL stream: legacy default stream
+        CUDA_CHECK(cudaEventRecord(last_done_, stream));
     }
 
     KernelTimer& timer() override { return timer_; }
@@ -815,8 +820,7 @@ private:
         for (int c = 0; c < 2; c++) {
             float* lin = plane(c, 0);
             if (!generic_) {
-                ingest_linear_kernel<<<(unsigned)ceil_div(n0, 256), 256, 0, st>>>(raw[c], cp[c], lin, plane_floats_);
-                CUDA_CHECK(cudaGetLastError());
+                launch_ingest_linear(raw[c], cp[c], lin, plane_floats_, st);
             } else {
                 lin_generic_[c].run(raw[c], cp[c], geo_[c], st);
                 const float* win = lin_generic_[c].planes + (int64_t)geo_[c].crop_top * geo_[c].TW + geo_[c].crop_left;
@@ -856,6 +860,10 @@ private:
         device_free(distmap_d_);
         pinned_free(norms_host_);
         pool_ = nullptr; partials_ = nullptr; norms_d_ = nullptr; distmap_d_ = nullptr; norms_host_ = nullptr;
+        if (last_done_) {
+            (void)cudaEventDestroy(last_done_);
+            last_done_ = nullptr;
+        }
         if (stream_) {
             (void)cudaStreamDestroy(stream_);
             stream_ = nullptr;
@@ -881,6 +889,7 @@ private:
     double* norms_d_ = nullptr;
     double* norms_host_ = nullptr;
     float* distmap_d_ = nullptr;
+    cudaEvent_t last_done_ = nullptr;  // completion of the previous call, on whichever stream it ran
     KernelTimer timer_;
 };
 

@@ -26,8 +26,8 @@ struct ColourParams {
     int bytes;           // bytes per stored sample
     unsigned mask;       // low-bit mask for 16-bit integer containers
     int misaligned;      // some stride is not a multiple of `bytes`: use byte loads
-    float full_norm;     // full range divisor (2^bits - 1, or 1 for float/half)
-    float lim_div;       // limited range: integer divisor 2^(bits-8) (0 for float/half)
+    float full_scale;    // full range: 1 / (2^bits - 1), or 1 for float/half
+    float lim_scale;     // limited range: 1 / 2^(bits-8), or 256 for float/half
     int full_range;
     int yuv_chroma;      // planes 1 and 2 are chroma (YUV family)
     int subw, subh;
@@ -69,14 +69,15 @@ __device__ __forceinline__ float load_norm(const uint8_t* plane, int64_t stride,
         if (cp.sample == Vship_SampleHALF) v = __half2float(__ushort_as_half(u));
         else v = (float)(u & cp.mask);
     }
+    // FullRange (rangeToFull.hpp:24-55) with the divisions applied as reciprocal products
+    // (at most one rounding apart from the reference's quotients).
     if (cp.full_range) {
-        v /= cp.full_norm;
+        v *= cp.full_scale;
         if (chroma) v -= 0.5f;
         return v;
     }
-    if (cp.lim_div > 0.f) v /= cp.lim_div;
-    else v *= 256.f;
-    return chroma ? (v - 128.f) / 224.f : (v - 16.f) / 219.f;
+    v *= cp.lim_scale;
+    return chroma ? (v - 128.f) * (1.0f / 224.f) : (v - 16.f) * (1.0f / 219.f);
 }
 
 // CubicHermitSplineInterpolator (src/gpuColorToLinear/resize.hpp:5-24).
@@ -203,11 +204,13 @@ __device__ __forceinline__ float trc_one(float a, int trc) {
         return a > -0.0228f ? 4 * a : (float)((double)(-1.1115f * powf(-a, 0.45f)) + 0.1115);
     case Vship_TRC_ST428: return (float)((double)signed_powf(a, 2.6f) * (52.37 / 48.));
     case Vship_TRC_PQ: {
-        const float m = 78.843750000000000f, n = 0.15930175781250000f;
-        const float c1 = 0.83593750000000000f, c2 = 18.851562500000000f, c3 = 18.687500000000000f;
-        a = fmaxf(0.f, a);
-        a = powf(a, 1.f / m);
-        return 100.f * powf(fmaxf(0.f, a - c1) / (c2 - c3 * a), 1.f / n);
+        // Evaluated in FP64: the EOTF subtracts c1 from a value near it and then raises to
+        // 1/n ~ 6.3, which turns FP32 rounding into ~1e-3 score errors on dark content.
+        const double m = 78.843750000000000, n = 0.15930175781250000;
+        const double c1 = 0.83593750000000000, c2 = 18.851562500000000, c3 = 18.687500000000000;
+        double x = fmax(0.0, (double)a);
+        x = pow(x, 1.0 / m);
+        return (float)(100.0 * pow(fmax(0.0, x - c1) / (c2 - c3 * x), 1.0 / n));
     }
     default: return a;
     }
@@ -215,14 +218,15 @@ __device__ __forceinline__ float trc_one(float a, int trc) {
 
 __device__ __forceinline__ float3 transfer(float3 v, int trc) {
     if (trc == Vship_TRC_HLG) {
-        const float a = 0.17883277f, b = 1.f - 4.f * a, c = 0.5f - a * -0.3350097945111627f;
-        v.x = v.x <= 0.5f ? v.x * v.x / 3.f : (expf((v.x - c) / a) + b) / 12.f;
-        v.y = v.y <= 0.5f ? v.y * v.y / 3.f : (expf((v.y - c) / a) + b) / 12.f;
-        v.z = v.z <= 0.5f ? v.z * v.z / 3.f : (expf((v.z - c) / a) + b) / 12.f;
-        const float ys = (float)((double)(0.2627f * v.x + 0.6780f * v.y) + 0.0593 * (double)v.z);
-        const float s = powf(ys, 1.2f - 1.f);
-        v.x *= s; v.y *= s; v.z *= s;
-        return v;
+        // Inverse OETF and OOTF of HLG, in FP64 for the same reason as PQ.
+        const double a = 0.17883277, b = 1.0 - 4.0 * a, c = 0.5 - a * -0.3350097945111627;
+        double x = v.x, y = v.y, z = v.z;
+        x = x <= 0.5 ? x * x / 3.0 : (exp((x - c) / a) + b) / 12.0;
+        y = y <= 0.5 ? y * y / 3.0 : (exp((y - c) / a) + b) / 12.0;
+        z = z <= 0.5 ? z * z / 3.0 : (exp((z - c) / a) + b) / 12.0;
+        const double ys = 0.2627 * x + 0.6780 * y + 0.0593 * z;
+        const double s = pow(ys, 1.2 - 1.0);
+        return make_float3((float)(x * s), (float)(y * s), (float)(z * s));
     }
     v.x = trc_one(v.x, trc);
     v.y = trc_one(v.y, trc);
@@ -260,18 +264,146 @@ __device__ __forceinline__ float3 primaries_to_709(float3 v, int prim) {
     return mat3f(v, 3.2410f, -1.5374f, -0.4986f, -0.9692f, 1.8760f, 0.0416f, 0.0556f, -0.2040f, 1.0570f);
 }
 
-// Linear BT.709 RGB of luma position (X, Y) of one raw image.
-__device__ __forceinline__ float3 ingest_pixel(const RawImage& im, int64_t X, int64_t Y, const ColourParams& cp) {
-    float3 v;
-    v.x = load_norm(im.p[0], im.stride[0], X, Y, cp, false);
-    v.y = chroma_at(im, 1, X, Y, cp);
-    v.z = chroma_at(im, 2, X, Y, cp);
+// ---------------------------------------------------------------------------------------
+// Tile-staged chroma: a CTA working on luma tile [X0, X0+64) x [Y0, Y0+64) decodes each
+// chroma sample it needs once into shared memory (S), interpolates horizontally once per
+// (chroma row, luma column) (HH), and then every pixel only does the vertical step.
+// ---------------------------------------------------------------------------------------
+constexpr int kStageTile = 64;
+
+struct ChromaStage {
+    int cx_lo, cx_n;  // staged chroma columns [cx_lo, cx_lo + cx_n)
+    int cy_lo, cy_n;  // staged chroma rows
+    float* S;         // [2][cy_n][cx_n]  decoded, range-normalised samples
+    float* HH;        // [2][cy_n][64]    horizontally interpolated at each luma column
+};
+
+// Floats of shared memory chroma_stage() needs for a colourspace (0 when not subsampled).
+__host__ __device__ inline int chroma_stage_floats(int subw, int subh) {
+    if (subw == 0 && subh == 0) return 0;
+    const int rows = subh ? (kStageTile >> subh) + 5 : kStageTile;
+    const int cols = subw ? (kStageTile >> subw) + 5 : kStageTile;
+    return 2 * rows * cols + 2 * rows * kStageTile;
+}
+
+__device__ __forceinline__ void chroma_stage(const RawImage& im, const ColourParams& cp, int X0, int Y0, float* smem,
+                                             ChromaStage& st) {
+    const int Xl = (int)min((int64_t)X0 + kStageTile - 1, cp.W - 1);
+    const int Yl = (int)min((int64_t)Y0 + kStageTile - 1, cp.H - 1);
+    int64_t i0, i1;
+    float t;
+    if (cp.subw) {
+        upsample_phase(X0, cp.subw, cp.hcenter, i0, t);
+        upsample_phase(Xl, cp.subw, cp.hcenter, i1, t);
+        st.cx_lo = (int)clamp64(i0 - 1, 0, cp.cw - 1);
+        st.cx_n = (int)clamp64(i1 + 2, 0, cp.cw - 1) - st.cx_lo + 1;
+    } else {
+        st.cx_lo = X0;
+        st.cx_n = Xl - X0 + 1;
+    }
+    if (cp.subh) {
+        upsample_phase(Y0, cp.subh, cp.vcenter, i0, t);
+        upsample_phase(Yl, cp.subh, cp.vcenter, i1, t);
+        st.cy_lo = (int)clamp64(i0 - 1, 0, cp.ch - 1);
+        st.cy_n = (int)clamp64(i1 + 2, 0, cp.ch - 1) - st.cy_lo + 1;
+    } else {
+        st.cy_lo = Y0;
+        st.cy_n = Yl - Y0 + 1;
+    }
+    st.S = smem;
+    st.HH = smem + 2 * st.cy_n * st.cx_n;
+    const bool chroma = cp.yuv_chroma != 0;
+    const int ns = st.cy_n * st.cx_n;
+    for (int i = threadIdx.x; i < 2 * ns; i += blockDim.x) {
+        const int p = i / ns, rem = i - p * ns;
+        const int r = rem / st.cx_n, c = rem - r * st.cx_n;
+        st.S[i] = load_norm(im.p[1 + p], im.stride[1 + p], st.cx_lo + c, st.cy_lo + r, cp, chroma);
+    }
+    __syncthreads();
+    const int nh = st.cy_n * kStageTile;
+    for (int i = threadIdx.x; i < 2 * nh; i += blockDim.x) {
+        const int p = i / nh, rem = i - p * nh;
+        const int r = rem / kStageTile, x = rem - r * kStageTile;
+        const int X = X0 + x;
+        if (X > Xl) continue;
+        const float* row = st.S + p * ns + r * st.cx_n;
+        float v;
+        if (cp.subw) {
+            int64_t ix;
+            float tx;
+            upsample_phase(X, cp.subw, cp.hcenter, ix, tx);
+            const float em1 = row[clamp64(ix - 1, 0, cp.cw - 1) - st.cx_lo];
+            const float e0 = row[clamp64(ix, 0, cp.cw - 1) - st.cx_lo];
+            const float e1 = row[clamp64(ix + 1, 0, cp.cw - 1) - st.cx_lo];
+            const float e2 = row[clamp64(ix + 2, 0, cp.cw - 1) - st.cx_lo];
+            v = hermite(e0, (e1 - em1) / 2, e1, (e2 - e0) / 2, tx);
+        } else {
+            v = row[X - st.cx_lo];
+        }
+        st.HH[i] = v;
+    }
+    __syncthreads();
+}
+
+// Both chroma values at luma (X, Y) of the staged tile whose origin is X0.
+__device__ __forceinline__ float2 chroma_from_stage(const ChromaStage& st, const ColourParams& cp, int X, int Y, int X0) {
+    const int x = X - X0;
+    const int nh = st.cy_n * kStageTile;
+    if (!cp.subh) {
+        const int r = Y - st.cy_lo;
+        return make_float2(st.HH[r * kStageTile + x], st.HH[nh + r * kStageTile + x]);
+    }
+    int64_t iy;
+    float ty;
+    upsample_phase(Y, cp.subh, cp.vcenter, iy, ty);
+    const int r0 = (int)clamp64(iy - 1, 0, cp.ch - 1) - st.cy_lo, r1 = (int)clamp64(iy, 0, cp.ch - 1) - st.cy_lo;
+    const int r2 = (int)clamp64(iy + 1, 0, cp.ch - 1) - st.cy_lo, r3 = (int)clamp64(iy + 2, 0, cp.ch - 1) - st.cy_lo;
+    float out[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const float* col = st.HH + p * nh + x;
+        const float h0 = col[r0 * kStageTile], h1 = col[r1 * kStageTile];
+        const float h2 = col[r2 * kStageTile], h3 = col[r3 * kStageTile];
+        out[p] = hermite(h1, (h2 - h0) / 2, h2, (h3 - h1) / 2, ty);
+    }
+    return make_float2(out[0], out[1]);
+}
+
+// Y'CbCr (or R'G'B') -> linear BT.709 RGB of one pixel.
+__device__ __forceinline__ float3 to_linear_709(float3 v, const ColourParams& cp) {
     if (!cp.skip_yuv) {
         v = gamma_light(v, cp.matrix);
         v = transfer(v, cp.trc);
         v = linear_light(v, cp.matrix);
     }
     return primaries_to_709(v, cp.primaries);
+}
+
+// Linear BT.709 RGB of luma (X, Y) inside a tile prepared by chroma_stage (or any pixel when
+// the clip is not chroma-subsampled).
+__device__ __forceinline__ float3 ingest_staged(const RawImage& im, const ColourParams& cp, const ChromaStage& st,
+                                               int X, int Y, int X0) {
+    float3 v;
+    v.x = load_norm(im.p[0], im.stride[0], X, Y, cp, false);
+    if (cp.subw == 0 && cp.subh == 0) {
+        const bool chroma = cp.yuv_chroma != 0;
+        v.y = load_norm(im.p[1], im.stride[1], X, Y, cp, chroma);
+        v.z = load_norm(im.p[2], im.stride[2], X, Y, cp, chroma);
+    } else {
+        const float2 c = chroma_from_stage(st, cp, X, Y, X0);
+        v.y = c.x;
+        v.z = c.y;
+    }
+    return to_linear_709(v, cp);
+}
+
+// Linear BT.709 RGB of luma position (X, Y) of one raw image.
+__device__ __forceinline__ float3 ingest_pixel(const RawImage& im, int64_t X, int64_t Y, const ColourParams& cp) {
+    float3 v;
+    v.x = load_norm(im.p[0], im.stride[0], X, Y, cp, false);
+    v.y = chroma_at(im, 1, X, Y, cp);
+    v.z = chroma_at(im, 2, X, Y, cp);
+    return to_linear_709(v, cp);
 }
 
 }  // namespace vship

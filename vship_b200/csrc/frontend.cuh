@@ -85,8 +85,8 @@ inline ColourParams make_colour_params(const Vship_Colorspace_t& cs, const ClipG
     cp.mask = bits >= 16 ? 0xFFFFu : ((1u << bits) - 1u);
     cp.misaligned = misaligned ? 1 : 0;
     cp.full_range = cs.range == Vship_RangeFull;
-    cp.full_norm = (float)((1 << bits) - 1);
-    cp.lim_div = bits >= 8 ? (float)(1 << (bits - 8)) : 0.f;
+    cp.full_scale = 1.0f / (float)((1 << bits) - 1);
+    cp.lim_scale = bits >= 8 ? 1.0f / (float)(1 << (bits - 8)) : 256.f;
     cp.yuv_chroma = cs.colorFamily == Vship_ColorYUV;
     cp.subw = cs.subsampling.subw;
     cp.subh = cs.subsampling.subh;
@@ -132,14 +132,30 @@ inline void stage_host_image(uint8_t* dst, const int64_t plane_off[3], const Cli
 // ---- generic path: ingest to planar linear RGB, then resize (horizontalResizeTranspose,
 // ---- src/gpuColorToLinear/resize.hpp:26-48), crop by offset.
 
-static __global__ void ingest_linear_kernel(RawImage im, ColourParams cp, float* out, int64_t plane_stride) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= cp.W * cp.H) return;
-    const int64_t X = i % cp.W, Y = i / cp.W;
-    const float3 v = ingest_pixel(im, X, Y, cp);
-    out[i] = v.x;
-    out[plane_stride + i] = v.y;
-    out[2 * plane_stride + i] = v.z;
+// Planar linear RGB of one image, one 64x64 luma tile per CTA with its chroma staged in
+// shared memory (dynamic: chroma_stage_floats(subw, subh) floats).
+static __global__ void __launch_bounds__(256) ingest_linear_kernel(RawImage im, ColourParams cp, float* out, int64_t plane_stride) {
+    extern __shared__ float stage_mem[];
+    const int X0 = blockIdx.x * kStageTile, Y0 = blockIdx.y * kStageTile;
+    ChromaStage st{};
+    if (cp.subw || cp.subh) chroma_stage(im, cp, X0, Y0, stage_mem, st);
+    for (int i = threadIdx.x; i < kStageTile * kStageTile; i += blockDim.x) {
+        const int X = X0 + (i & (kStageTile - 1)), Y = Y0 + i / kStageTile;
+        if (X >= cp.W || Y >= cp.H) continue;
+        const float3 v = ingest_staged(im, cp, st, X, Y, X0);
+        const int64_t o = (int64_t)Y * cp.W + X;
+        out[o] = v.x;
+        out[plane_stride + o] = v.y;
+        out[2 * plane_stride + o] = v.z;
+    }
+}
+
+inline void launch_ingest_linear(const RawImage& im, const ColourParams& cp, float* out, int64_t plane_stride, cudaStream_t st) {
+    const dim3 grid((unsigned)ceil_div(cp.W, kStageTile), (unsigned)ceil_div(cp.H, kStageTile));
+    const size_t smem = sizeof(float) * chroma_stage_floats(cp.subw, cp.subh);
+    if (smem > 48 * 1024) CUDA_CHECK(cudaFuncSetAttribute(ingest_linear_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ingest_linear_kernel<<<grid, 256, smem, st>>>(im, cp, out, plane_stride);
+    CUDA_CHECK(cudaGetLastError());
 }
 
 // One pass of the separable resize: rows of length sw resized to rw samples, written
@@ -179,8 +195,7 @@ struct GenericLinear {
         const int64_t n = g.W * g.H;
         float* lin = g.resized ? scratch : planes;
         const int64_t lin_stride = g.resized ? n : plane_floats;
-        ingest_linear_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, stream>>>(im, cp, lin, lin_stride);
-        CUDA_CHECK(cudaGetLastError());
+        launch_ingest_linear(im, cp, lin, lin_stride, stream);
         if (!g.resized) return;
         float* mid = scratch + 3 * n;
         for (int c = 0; c < 3; c++) {

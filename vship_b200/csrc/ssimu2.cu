@@ -10,9 +10,10 @@
 //                           built in shared memory; only planes some map reads are stored)
 //   2. ssimu2_maps_kernel   one launch over a work list of 32x32 output tiles of every
 //                           unpruned (pair, plane, scale): 48x48 halo tiles of both images,
-//                           separable 17-tap renormalised blur of a, b, ab and a^2+b^2 in
-//                           shared memory, SSIM / artifact / detail-loss maps, per-tile sums
-//                           of x and x^4 in FP64
+//                           separable 17-tap renormalised blur of a-k, b-k, (a-k)(b-k) and
+//                           (a-b)^2 in shared memory (k: a per-tile shift), SSIM / artifact /
+//                           detail-loss maps in a cancellation-free form, per-tile sums of x
+//                           and x^4 in FP64
 //   3. ssimu2_final_kernel  per pair: FP64 sum of tile partials, 4th roots, the 108 features
 //                           and the score, computed like the reference's final_score
 //
@@ -144,13 +145,16 @@ __global__ void __launch_bounds__(256) ssimu2_front_kernel(const __grid_constant
     const int pitch0 = a.pyr.pitch[0];
     float* y0plane = out + a.pyr.off[0][1];
     const RawImage& im = a.raw[img];
+    extern __shared__ float stage_mem[];
+    ChromaStage st{};
+    if (!FromLinear && (cp.subw || cp.subh)) chroma_stage(im, cp, blockIdx.x * kStageTile, blockIdx.y * kStageTile, stage_mem, st);
 
     auto pixel = [&](int X, int Y) -> float3 {
         if (FromLinear) {
             const float* base = a.lin[clip] + (int64_t)Y * a.lin_pitch[clip] + X;
             return make_float3(base[0], base[a.lin_plane[clip]], base[2 * a.lin_plane[clip]]);
         } else {
-            return ingest_pixel(im, X, Y, cp);
+            return ingest_staged(im, cp, st, X, Y, blockIdx.x * kStageTile);
         }
     };
 
@@ -245,15 +249,32 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
     const int X0 = (local % sg.tiles_x) * kTile, Y0 = (local / sg.tiles_x) * kTile;
     const int tid = threadIdx.x;
 
-    // Halo tiles of both images; zero outside the plane (src/ssimu2/gaussianblur.hpp:24-36).
+    // Moments are taken of values shifted by a per-tile constant k (the mean of both images
+    // at the tile's centre pixel).  The renormalised blur maps constants to themselves, so
+    // blur((a-k)^2) - blur(a-k)^2 equals the reference's blur(a^2) - blur(a)^2 exactly in
+    // real arithmetic, while in FP32 it no longer cancels ~0.25-sized terms down to the
+    // ~1e-5 local variances of smooth regions.  k is symmetric in the two images, so
+    // identical inputs still give bit-identical moments and an SSIM map of exactly 0.
+    __shared__ float s_shift;
+    if (tid == 0) {
+        const int cx = min(X0 + kTile / 2, sg.w - 1), cy = min(Y0 + kTile / 2, sg.h - 1);
+        const int64_t o = (int64_t)cy * sg.pitch + cx;
+        s_shift = 0.5f * (__ldg(sg.a + o) + __ldg(sg.b + o));
+    }
+    __syncthreads();
+    const float k = s_shift;
+
+    // Halo tiles of both images, shifted; zero outside the plane, as the reference's zero
+    // padding (src/ssimu2/gaussianblur.hpp:24-36): out-of-image taps add nothing and the
+    // renormalisation divides by the in-image tap weights only.
     for (int i = tid; i < kIn * kIn; i += 256) {
         const int r = i / kIn, c = i % kIn;
         const int gx = X0 - kHalo + c, gy = Y0 - kHalo + r;
         float va = 0.f, vb = 0.f;
         if (gx >= 0 && gx < sg.w && gy >= 0 && gy < sg.h) {
             const int64_t o = (int64_t)gy * sg.pitch + gx;
-            va = __ldg(sg.a + o);
-            vb = __ldg(sg.b + o);
+            va = __ldg(sg.a + o) - k;
+            vb = __ldg(sg.b + o) - k;
         }
         sa[r][c] = va;
         sb[r][c] = vb;
@@ -269,8 +290,9 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
         for (int j = 0; j < 18; j++) {
             av[j] = sa[r][c0 + j];
             bv[j] = sb[r][c0 + j];
-            pv[j] = __fmul_rn(av[j], bv[j]);
-            qv[j] = __fadd_rn(__fmul_rn(av[j], av[j]), __fmul_rn(bv[j], bv[j]));
+            pv[j] = av[j] * bv[j];
+            const float dj = av[j] - bv[j];
+            qv[j] = dj * dj;
         }
         float acc[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
 #pragma unroll
@@ -316,19 +338,23 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
         const int gy = Y0 + r0 + o;
         if (gx >= sg.w || gy >= sg.h) continue;
         const float tot = blur_norm(gy, sg.h);
-        const float m1 = mo[0][o] / tot, m2 = mo[1][o] / tot, s12 = mo[2][o] / tot, ssq = mo[3][o] / tot;
-        // SSIM map (src/ssimu2/score.hpp:266-274) with a^2+b^2 blurred directly; rounding is
-        // explicit so that identical inputs give exactly 0.
-        const float mu = __fmul_rn(m1, m2);
-        const float m11 = __fmul_rn(m1, m1), m22 = __fmul_rn(m2, m2);
-        const float md = __fsub_rn(m1, m2);
-        const float num_m = __fsub_rn(1.0f, __fmul_rn(md, md));
-        const float num_s = __fadd_rn(__fmul_rn(2.0f, __fsub_rn(s12, mu)), 0.0009f);
-        const float den_s = __fadd_rn(__fsub_rn(ssq, __fadd_rn(m11, m22)), 0.0009f);
-        const float ssim = fmaxf(1.0f - (num_m * num_s) / den_s, 0.0f);
-        // Artifact and detail-loss maps (score.hpp:276-281).
+        // Shifted means m1 = mu1 - k, m2 = mu2 - k, s12 = blur((a-k)(b-k)), D = blur((a-b)^2).
+        const float m1 = mo[0][o] / tot, m2 = mo[1][o] / tot, s12 = mo[2][o] / tot, D = mo[3][o] / tot;
+        // SSIM map of the reference (src/ssimu2/score.hpp:266-274),
+        //   ssim = 1 - (1 - md^2) * N / (s1^2 + s2^2 + C),  N = 2 s12' + C,  md = mu1 - mu2,
+        // rewritten without cancellation: with V = D - md^2 (the local variance of a - b),
+        // s1^2 + s2^2 + C = V + N and therefore ssim = (V + md^2 N) / (V + N).  Identical
+        // inputs give V = md = 0 and an SSIM of exactly 0.
+        const float md = m1 - m2;
+        const float md2 = md * md;
+        const float N = fmaf(2.0f, s12 - m1 * m2, 0.0009f);
+        const float V = D - md2;
+        const float ssim = fmaxf(fmaf(md2, N, V) / (V + N), 0.0f);
+        // Artifact and detail-loss maps (score.hpp:276-281): (|b-mu2|+1)/(|a-mu1|+1) - 1,
+        // evaluated as (|b-mu2| - |a-mu1|) / (|a-mu1| + 1) to avoid cancelling against 1.
         const float ca = sa[r0 + o + kHalo][c + kHalo], cb = sb[r0 + o + kHalo][c + kHalo];
-        const float v1 = (fabsf(cb - m2) + 1.0f) / (fabsf(ca - m1) + 1.0f) - 1.0f;
+        const float ea = fabsf(ca - m1), eb = fabsf(cb - m2);
+        const float v1 = (eb - ea) / (ea + 1.0f);
         const float art = fmaxf(v1, 0.0f), det = fmaxf(-v1, 0.0f);
         const float s2 = ssim * ssim, a2 = art * art, d2 = det * det;
         sum[0] += ssim; sum[1] += art; sum[2] += det;
@@ -441,6 +467,7 @@ public:
         generic_ = geo_[0].generic() || geo_[1].generic();
         build_pyramid();
         CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        CUDA_CHECK(cudaEventCreateWithFlags(&last_done_, cudaEventDisableTiming));
         upload_gauss_constants();
         for (int c = 0; c < 2; c++) {
             staged_bytes_[c] = dense_image_bytes(geo_[c], staged_off_[c]);
@@ -452,6 +479,7 @@ public:
     }
 
     double compute(const uint8_t* const s1[3], const uint8_t* const s2[3], const int64_t ls1[3], const int64_t ls2[3]) override {
+        CUDA_CHECK(cudaStreamWaitEvent(stream_, last_done_, 0));
         stage_host_image(staged_[0], staged_off_[0], geo_[0], s1, ls1, stream_);
         stage_host_image(staged_[1], staged_off_[1], geo_[1], s2, ls2, stream_);
         RawImage raw[2];
@@ -463,6 +491,7 @@ public:
         run_pairs(1, raw, cp_, stream_, scores_d_, features_d_);
         CUDA_CHECK(cudaMemcpyAsync(score_host_, scores_d_, sizeof(double), cudaMemcpyDeviceToHost, stream_));
         CUDA_CHECK(cudaMemcpyAsync(last_features_, features_d_, sizeof(float) * 108, cudaMemcpyDeviceToHost, stream_));
+        CUDA_CHECK(cudaEventRecord(last_done_, stream_));
         CUDA_CHECK(cudaStreamSynchronize(stream_));
         return *score_host_;
     }
@@ -484,7 +513,8 @@ public:
                 if (ls[p] % geo_[c].bytes) cp[c].misaligned = 1;
             }
         }
-        cudaStream_t st = stream ? stream : stream_;
+        cudaStream_t st = stream;  // NULL: the CUDA legacy default stream
+        CUDA_CHECK(cudaStreamWaitEvent(st, last_done_, 0));
         std::vector<RawImage> raw(2 * kMaxBatch);
         int done = 0;
         while (done < n) {
@@ -504,6 +534,7 @@ public:
                       d_features ? d_features + (int64_t)done * 108 : features_d_);
             done += chunk;
         }
+        CUDA_CHECK(cudaEventRecord(last_done_, st));
     }
 
     void last_features(float out[108]) override { std::memcpy(out, last_features_, sizeof(last_features_)); }
@@ -606,8 +637,12 @@ private:
         for (int i = 0; i < nimg; i++) fa->raw[i] = raw[i];
         const dim3 fgrid((unsigned)ceil_div(pyr_.w[1], 32), (unsigned)ceil_div(pyr_.h[1], 32), (unsigned)nimg);
         if (!generic_) {
+            const int smem = (int)sizeof(float) * std::max(chroma_stage_floats(cp[0].subw, cp[0].subh),
+                                                           chroma_stage_floats(cp[1].subw, cp[1].subh));
+            if (smem > 32 * 1024)
+                CUDA_CHECK(cudaFuncSetAttribute(ssimu2_front_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
             const int t = timer_.begin(0, "ssimu2_front", st);
-            ssimu2_front_kernel<false><<<fgrid, 256, 0, st>>>(*fa);
+            ssimu2_front_kernel<false><<<fgrid, 256, smem, st>>>(*fa);
             CUDA_CHECK(cudaGetLastError());
             timer_.end(t, st);
         } else {
@@ -649,6 +684,10 @@ private:
         pinned_free(score_host_);
         xyb_ = nullptr; partials_ = nullptr; segs_d_ = nullptr; scores_d_ = nullptr; features_d_ = nullptr;
         score_host_ = nullptr;
+        if (last_done_) {
+            (void)cudaEventDestroy(last_done_);
+            last_done_ = nullptr;
+        }
         if (stream_) {
             (void)cudaStreamDestroy(stream_);
             stream_ = nullptr;
@@ -677,6 +716,7 @@ private:
     float last_features_[108] = {};
     int cap_ = 0;
     FrontArgs front_args_{};
+    cudaEvent_t last_done_ = nullptr;  // completion of the previous call, on whichever stream it ran
     KernelTimer timer_;
 };
 

@@ -37,7 +37,7 @@ def sinusoid_field(rng, w, h, count=32, pmin=4.0, pmax=512.0):
         u = min(u, w // 2)
         v %= h
         if u == 0 and v == 0:
-            u = 1
+            continue
         amp = rng.uniform(2.0, 14.0)
         phase = rng.uniform(0, 2 * np.pi)
         spec[v, u] += amp * np.exp(1j * phase) * (w * h) / (2.0 if 0 < u < w / 2 else 1.0)
