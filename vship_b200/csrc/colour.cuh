@@ -137,14 +137,15 @@ __device__ __forceinline__ float chroma_at(const RawImage& im, int c, int64_t X,
 }
 
 // Non-constant-luminance Y'CbCr -> R'G'B' (YUVToLinRGB.hpp:7-18).
+// The three divisors are constants of the matrix; they are applied as reciprocal products.
 __device__ __forceinline__ float3 ncl_to_rgb(float3 v, const float kr, const float kb) {
     const float kg = 1.f - kb - kr;
     const float us = 0.5f / (1.f - kb);
     const float vs = 0.5f / (1.f - kr);
     float3 r;
-    r.x = (v.z + v.x * vs) / (vs * kr + 0.5f);
-    r.z = (v.y + v.x * us) / (us * kb + 0.5f);
-    r.y = (v.x - kr * r.x - kb * r.z) / kg;
+    r.x = (v.z + v.x * vs) * (1.0f / (vs * kr + 0.5f));
+    r.z = (v.y + v.x * us) * (1.0f / (us * kb + 0.5f));
+    r.y = (v.x - kr * r.x - kb * r.z) * (1.0f / kg);
     return r;
 }
 
@@ -184,25 +185,29 @@ __device__ __forceinline__ float3 linear_light(float3 v, int matrix) {
     return v;
 }
 
-__device__ __forceinline__ float signed_powf(float a, float g) { return a < 0 ? -powf(-a, g) : powf(a, g); }
+// |a|^g with the sign of a, as exp2(g * log2|a|) on the special-function unit.  The relative
+// error is ~3e-7 (log2 to 2^-21, exp2 to 2 ulp, times g), far below the metric's
+// resolution; pow's exact corner cases are not needed for finite pixel values.
+__device__ __forceinline__ float fast_pow(float x, float g) { return x > 0.f ? exp2f(g * __log2f(x)) : 0.f; }
+__device__ __forceinline__ float signed_powf(float a, float g) { return a < 0 ? -fast_pow(-a, g) : fast_pow(a, g); }
 
 __device__ __forceinline__ float trc_one(float a, int trc) {
     switch (trc) {
     case Vship_TRC_sRGB:
         if (a < 0) {
-            if (a < -0.04045f) return -powf((float)((-(double)a + 0.055) * (1.0 / 1.055)), 2.4f);
-            return (float)((double)a * (1.0 / 12.92));
+            if (a < -0.04045f) return -fast_pow((-a + 0.055f) * (1.0f / 1.055f), 2.4f);
+            return a * (1.0f / 12.92f);
         }
-        if (a > 0.04045f) return powf((float)(((double)a + 0.055) * (1.0 / 1.055)), 2.4f);
-        return (float)((double)a * (1.0 / 12.92));
+        if (a > 0.04045f) return fast_pow((a + 0.055f) * (1.0f / 1.055f), 2.4f);
+        return a * (1.0f / 12.92f);
     case Vship_TRC_BT709: return signed_powf(a, 2.4f);
     case Vship_TRC_BT470_M: return signed_powf(a, 2.2f);
     case Vship_TRC_BT470_BG:
     case Vship_TRC_BT601: return signed_powf(a, 2.8f);
     case Vship_TRC_ST240_M:
-        if (a >= 0) return a < 0.0228f ? 4 * a : (float)((double)(1.1115f * powf(a, 0.45f)) - 0.1115);
-        return a > -0.0228f ? 4 * a : (float)((double)(-1.1115f * powf(-a, 0.45f)) + 0.1115);
-    case Vship_TRC_ST428: return (float)((double)signed_powf(a, 2.6f) * (52.37 / 48.));
+        if (a >= 0) return a < 0.0228f ? 4 * a : 1.1115f * fast_pow(a, 0.45f) - 0.1115f;
+        return a > -0.0228f ? 4 * a : -1.1115f * fast_pow(-a, 0.45f) + 0.1115f;
+    case Vship_TRC_ST428: return signed_powf(a, 2.6f) * (float)(52.37 / 48.);
     case Vship_TRC_PQ: {
         // Evaluated in FP64: the EOTF subtracts c1 from a value near it and then raises to
         // 1/n ~ 6.3, which turns FP32 rounding into ~1e-3 score errors on dark content.
@@ -266,105 +271,129 @@ __device__ __forceinline__ float3 primaries_to_709(float3 v, int prim) {
 
 // ---------------------------------------------------------------------------------------
 // Tile-staged chroma: a CTA working on luma tile [X0, X0+64) x [Y0, Y0+64) decodes each
-// chroma sample it needs once into shared memory (S), interpolates horizontally once per
-// (chroma row, luma column) (HH), and then every pixel only does the vertical step.
+// chroma sample it needs once into shared memory (S, with the edge replication of the
+// reference's clamped interpolators baked in), interpolates horizontally once per (chroma
+// row, luma column) into HH, and every pixel then does only the vertical step.  Interval
+// starts and fractions of the tile's 64 columns and rows come from small phase tables.
 // ---------------------------------------------------------------------------------------
 constexpr int kStageTile = 64;
+constexpr int kStageMaxSpan = kStageTile + 4;  // staged rows/columns: interval range + 3 taps
 
 struct ChromaStage {
-    int cx_lo, cx_n;  // staged chroma columns [cx_lo, cx_lo + cx_n)
-    int cy_lo, cy_n;  // staged chroma rows
-    float* S;         // [2][cy_n][cx_n]  decoded, range-normalised samples
-    float* HH;        // [2][cy_n][64]    horizontally interpolated at each luma column
+    int cx_lo, cx_n;     // staged chroma columns [cx_lo, cx_lo + cx_n) (may start below 0)
+    int cy_lo, cy_n;     // staged chroma rows
+    float* S;            // [2][cy_n][kStageMaxSpan] decoded, range-normalised samples
+    float* HH;           // [2][cy_n][64] horizontally interpolated at each luma column
+    short* hb;           // [64] S column of the first tap of luma column x
+    float* ht;           // [64] horizontal fraction of luma column x
+    short* vb;           // [64] HH row of the first tap of luma row y
+    float* vt;           // [64] vertical fraction of luma row y
 };
 
 // Floats of shared memory chroma_stage() needs for a colourspace (0 when not subsampled).
 __host__ __device__ inline int chroma_stage_floats(int subw, int subh) {
     if (subw == 0 && subh == 0) return 0;
     const int rows = subh ? (kStageTile >> subh) + 5 : kStageTile;
-    const int cols = subw ? (kStageTile >> subw) + 5 : kStageTile;
-    return 2 * rows * cols + 2 * rows * kStageTile;
+    return 2 * rows * kStageMaxSpan + 2 * rows * kStageTile + 4 * kStageTile;
+}
+
+// Interval start and fraction of output sample X on an axis decimated by 2^sub (int32).
+__device__ __forceinline__ void phase32(int X, int sub, int centered, int& i, float& t) {
+    if (sub == 0) { i = X; t = 0.f; return; }
+    const int f = 1 << sub;
+    if (!centered) {
+        i = X >> sub;
+        t = (float)(X & (f - 1)) * (1.0f / (float)f);
+    } else {
+        const int off = X - (f >> 1);
+        i = off >> sub;  // arithmetic shift: floor division
+        t = ((float)(off - (i << sub)) + 0.5f) * (1.0f / (float)f);
+    }
 }
 
 __device__ __forceinline__ void chroma_stage(const RawImage& im, const ColourParams& cp, int X0, int Y0, float* smem,
                                              ChromaStage& st) {
-    const int Xl = (int)min((int64_t)X0 + kStageTile - 1, cp.W - 1);
-    const int Yl = (int)min((int64_t)Y0 + kStageTile - 1, cp.H - 1);
-    int64_t i0, i1;
+    const int W = (int)cp.W, H = (int)cp.H, cw = (int)cp.cw, ch = (int)cp.ch;
+    const int Xl = min(X0 + kStageTile - 1, W - 1), Yl = min(Y0 + kStageTile - 1, H - 1);
+    int i0, i1;
     float t;
     if (cp.subw) {
-        upsample_phase(X0, cp.subw, cp.hcenter, i0, t);
-        upsample_phase(Xl, cp.subw, cp.hcenter, i1, t);
-        st.cx_lo = (int)clamp64(i0 - 1, 0, cp.cw - 1);
-        st.cx_n = (int)clamp64(i1 + 2, 0, cp.cw - 1) - st.cx_lo + 1;
+        phase32(X0, cp.subw, cp.hcenter, i0, t);
+        phase32(Xl, cp.subw, cp.hcenter, i1, t);
+        st.cx_lo = i0 - 1;
+        st.cx_n = i1 + 3 - st.cx_lo;
     } else {
         st.cx_lo = X0;
         st.cx_n = Xl - X0 + 1;
     }
     if (cp.subh) {
-        upsample_phase(Y0, cp.subh, cp.vcenter, i0, t);
-        upsample_phase(Yl, cp.subh, cp.vcenter, i1, t);
-        st.cy_lo = (int)clamp64(i0 - 1, 0, cp.ch - 1);
-        st.cy_n = (int)clamp64(i1 + 2, 0, cp.ch - 1) - st.cy_lo + 1;
+        phase32(Y0, cp.subh, cp.vcenter, i0, t);
+        phase32(Yl, cp.subh, cp.vcenter, i1, t);
+        st.cy_lo = i0 - 1;
+        st.cy_n = i1 + 3 - st.cy_lo;
     } else {
         st.cy_lo = Y0;
         st.cy_n = Yl - Y0 + 1;
     }
     st.S = smem;
-    st.HH = smem + 2 * st.cy_n * st.cx_n;
+    st.HH = st.S + 2 * st.cy_n * kStageMaxSpan;
+    st.ht = st.HH + 2 * st.cy_n * kStageTile;
+    st.vt = st.ht + kStageTile;
+    st.hb = reinterpret_cast<short*>(st.vt + kStageTile);
+    st.vb = st.hb + kStageTile;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    if (tid < kStageTile) {
+        int i;
+        float f;
+        phase32(X0 + tid, cp.subw, cp.hcenter, i, f);
+        st.hb[tid] = (short)(cp.subw ? i - 1 - st.cx_lo : i - st.cx_lo);
+        st.ht[tid] = f;
+    } else if (tid < 2 * kStageTile) {
+        int i;
+        float f;
+        phase32(Y0 + tid - kStageTile, cp.subh, cp.vcenter, i, f);
+        st.vb[tid - kStageTile] = (short)(cp.subh ? i - 1 - st.cy_lo : i - st.cy_lo);
+        st.vt[tid - kStageTile] = f;
+    }
     const bool chroma = cp.yuv_chroma != 0;
-    const int ns = st.cy_n * st.cx_n;
-    for (int i = threadIdx.x; i < 2 * ns; i += blockDim.x) {
-        const int p = i / ns, rem = i - p * ns;
-        const int r = rem / st.cx_n, c = rem - r * st.cx_n;
-        st.S[i] = load_norm(im.p[1 + p], im.stride[1 + p], st.cx_lo + c, st.cy_lo + r, cp, chroma);
+    for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
+        const int p = r >= st.cy_n, rr = r - p * st.cy_n;
+        const int gy = min(max(st.cy_lo + rr, 0), ch - 1);
+        for (int c = lane; c < st.cx_n; c += 32) {
+            const int gx = min(max(st.cx_lo + c, 0), cw - 1);
+            st.S[r * kStageMaxSpan + c] = load_norm(im.p[1 + p], im.stride[1 + p], gx, gy, cp, chroma);
+        }
     }
     __syncthreads();
-    const int nh = st.cy_n * kStageTile;
-    for (int i = threadIdx.x; i < 2 * nh; i += blockDim.x) {
-        const int p = i / nh, rem = i - p * nh;
-        const int r = rem / kStageTile, x = rem - r * kStageTile;
-        const int X = X0 + x;
-        if (X > Xl) continue;
-        const float* row = st.S + p * ns + r * st.cx_n;
-        float v;
-        if (cp.subw) {
-            int64_t ix;
-            float tx;
-            upsample_phase(X, cp.subw, cp.hcenter, ix, tx);
-            const float em1 = row[clamp64(ix - 1, 0, cp.cw - 1) - st.cx_lo];
-            const float e0 = row[clamp64(ix, 0, cp.cw - 1) - st.cx_lo];
-            const float e1 = row[clamp64(ix + 1, 0, cp.cw - 1) - st.cx_lo];
-            const float e2 = row[clamp64(ix + 2, 0, cp.cw - 1) - st.cx_lo];
-            v = hermite(e0, (e1 - em1) / 2, e1, (e2 - e0) / 2, tx);
-        } else {
-            v = row[X - st.cx_lo];
+    for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
+        const float* row = st.S + r * kStageMaxSpan;
+        for (int x = lane; x < kStageTile; x += 32) {
+            const int j = st.hb[x];
+            float v;
+            if (cp.subw) {
+                const float em1 = row[j], e0 = row[j + 1], e1 = row[j + 2], e2 = row[j + 3];
+                v = hermite(e0, (e1 - em1) / 2, e1, (e2 - e0) / 2, st.ht[x]);
+            } else {
+                v = row[min(j, st.cx_n - 1)];
+            }
+            st.HH[r * kStageTile + x] = v;
         }
-        st.HH[i] = v;
     }
     __syncthreads();
 }
 
-// Both chroma values at luma (X, Y) of the staged tile whose origin is X0.
-__device__ __forceinline__ float2 chroma_from_stage(const ChromaStage& st, const ColourParams& cp, int X, int Y, int X0) {
-    const int x = X - X0;
+// Both chroma values at tile-local luma (x, y) of a tile prepared by chroma_stage.
+__device__ __forceinline__ float2 chroma_from_stage(const ChromaStage& st, const ColourParams& cp, int x, int y) {
     const int nh = st.cy_n * kStageTile;
-    if (!cp.subh) {
-        const int r = Y - st.cy_lo;
-        return make_float2(st.HH[r * kStageTile + x], st.HH[nh + r * kStageTile + x]);
-    }
-    int64_t iy;
-    float ty;
-    upsample_phase(Y, cp.subh, cp.vcenter, iy, ty);
-    const int r0 = (int)clamp64(iy - 1, 0, cp.ch - 1) - st.cy_lo, r1 = (int)clamp64(iy, 0, cp.ch - 1) - st.cy_lo;
-    const int r2 = (int)clamp64(iy + 1, 0, cp.ch - 1) - st.cy_lo, r3 = (int)clamp64(iy + 2, 0, cp.ch - 1) - st.cy_lo;
+    const int j = st.vb[y];
+    if (!cp.subh) return make_float2(st.HH[j * kStageTile + x], st.HH[nh + j * kStageTile + x]);
+    const float t = st.vt[y];
     float out[2];
 #pragma unroll
     for (int p = 0; p < 2; p++) {
-        const float* col = st.HH + p * nh + x;
-        const float h0 = col[r0 * kStageTile], h1 = col[r1 * kStageTile];
-        const float h2 = col[r2 * kStageTile], h3 = col[r3 * kStageTile];
-        out[p] = hermite(h1, (h2 - h0) / 2, h2, (h3 - h1) / 2, ty);
+        const float* col = st.HH + p * nh + j * kStageTile + x;
+        const float h0 = col[0], h1 = col[kStageTile], h2 = col[2 * kStageTile], h3 = col[3 * kStageTile];
+        out[p] = hermite(h1, (h2 - h0) / 2, h2, (h3 - h1) / 2, t);
     }
     return make_float2(out[0], out[1]);
 }
@@ -379,10 +408,10 @@ __device__ __forceinline__ float3 to_linear_709(float3 v, const ColourParams& cp
     return primaries_to_709(v, cp.primaries);
 }
 
-// Linear BT.709 RGB of luma (X, Y) inside a tile prepared by chroma_stage (or any pixel when
-// the clip is not chroma-subsampled).
+// Linear BT.709 RGB of luma (X, Y) inside the tile with origin (X0, Y0) prepared by
+// chroma_stage (or of any pixel when the clip is not chroma-subsampled).
 __device__ __forceinline__ float3 ingest_staged(const RawImage& im, const ColourParams& cp, const ChromaStage& st,
-                                               int X, int Y, int X0) {
+                                               int X, int Y, int X0, int Y0) {
     float3 v;
     v.x = load_norm(im.p[0], im.stride[0], X, Y, cp, false);
     if (cp.subw == 0 && cp.subh == 0) {
@@ -390,7 +419,7 @@ __device__ __forceinline__ float3 ingest_staged(const RawImage& im, const Colour
         v.y = load_norm(im.p[1], im.stride[1], X, Y, cp, chroma);
         v.z = load_norm(im.p[2], im.stride[2], X, Y, cp, chroma);
     } else {
-        const float2 c = chroma_from_stage(st, cp, X, Y, X0);
+        const float2 c = chroma_from_stage(st, cp, X - X0, Y - Y0);
         v.y = c.x;
         v.z = c.y;
     }

@@ -142,7 +142,7 @@ static __global__ void __launch_bounds__(256) ingest_linear_kernel(RawImage im, 
     for (int i = threadIdx.x; i < kStageTile * kStageTile; i += blockDim.x) {
         const int X = X0 + (i & (kStageTile - 1)), Y = Y0 + i / kStageTile;
         if (X >= cp.W || Y >= cp.H) continue;
-        const float3 v = ingest_staged(im, cp, st, X, Y, X0);
+        const float3 v = ingest_staged(im, cp, st, X, Y, X0, Y0);
         const int64_t o = (int64_t)Y * cp.W + X;
         out[o] = v.x;
         out[plane_stride + o] = v.y;

@@ -59,6 +59,15 @@ __constant__ float c_gauss[17];
 __constant__ float c_gauss_prefix[18];
 __constant__ double c_weights[108] = {VSHIP_SSIMU2_WEIGHT_LIST};
 
+// Cube root of max(x, 0): exp2(log2(x) / 3) on the special-function unit refined by one
+// Newton step y <- (2y + x / y^2) / 3, which leaves ~1 ulp of error.
+__device__ __forceinline__ float fast_cbrt(float x) {
+    if (!(x > 0.f)) return 0.f;
+    float y = exp2f(__log2f(x) * (1.0f / 3.0f));
+    y = (2.0f * y + __fdividef(x, y * y)) * (1.0f / 3.0f);
+    return y;
+}
+
 // positive XYB of a linear RGB triple (src/ssimu2/makeXYB.hpp:6-47).
 __device__ __forceinline__ float3 positive_xyb(float3 a) {
     const float bias = 0.0037930734f;
@@ -66,15 +75,17 @@ __device__ __forceinline__ float3 positive_xyb(float3 a) {
     float m = fmaf(0.23f, a.x, fmaf(0.692f, a.y, fmaf(0.078f, a.z, bias)));
     float s = fmaf(0.24342269f, a.x, fmaf(0.20476745f, a.y, fmaf(0.55180986f, a.z, bias)));
     const float absb = -0.1559542025327239f;
-    l = cbrtf(fmaxf(l, 0.f)) + absb;
-    m = cbrtf(fmaxf(m, 0.f)) + absb;
-    s = cbrtf(fmaxf(s, 0.f)) + absb;
+    l = fast_cbrt(l) + absb;
+    m = fast_cbrt(m) + absb;
+    s = fast_cbrt(s) + absb;
     const float X = 0.5f * (l - m);
     const float Y = X + m;
+    // make_positive_xyb (makeXYB.hpp:32-36); the reference adds the offsets in double,
+    // here in float (the stored value differs by at most one rounding).
     float3 r;
-    r.z = (float)((double)(s - Y) + 0.55);
-    r.x = (float)((double)(X * 14.0f) + 0.42);
-    r.y = (float)((double)Y + 0.01);
+    r.z = (s - Y) + 0.55f;
+    r.x = fmaf(X, 14.0f, 0.42f);
+    r.y = Y + 0.01f;
     return r;
 }
 
@@ -154,7 +165,7 @@ __global__ void __launch_bounds__(256) ssimu2_front_kernel(const __grid_constant
             const float* base = a.lin[clip] + (int64_t)Y * a.lin_pitch[clip] + X;
             return make_float3(base[0], base[a.lin_plane[clip]], base[2 * a.lin_plane[clip]]);
         } else {
-            return ingest_staged(im, cp, st, X, Y, blockIdx.x * kStageTile);
+            return ingest_staged(im, cp, st, X, Y, blockIdx.x * kStageTile, blockIdx.y * kStageTile);
         }
     };
 
@@ -226,15 +237,19 @@ __device__ __forceinline__ float blur_norm(int pos, int n) {
     return c_gauss_prefix[end] - c_gauss_prefix[beg];
 }
 
-__global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restrict__ segs, int nseg,
-                                                          double* __restrict__ partials) {
+constexpr int kMapThreads = 128;
+
+__global__ void __launch_bounds__(kMapThreads) ssimu2_maps_kernel(const MapSeg* __restrict__ segs, int nseg,
+                                                                  double* __restrict__ partials) {
     __shared__ float sa[kIn][kIn + 1];
     __shared__ float sb[kIn][kIn + 1];
     __shared__ float sh[4][kIn][kTile + 1];
-    __shared__ double red[8][6];
+    __shared__ double red[kMapThreads / 32][6];
     __shared__ int s_seg;
+    __shared__ float s_shift;
 
-    if (threadIdx.x == 0) {
+    const int tid = threadIdx.x;
+    if (tid == 0) {
         int lo = 0, hi = nseg - 1;
         const int t = blockIdx.x;
         while (lo < hi) {
@@ -247,15 +262,13 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
     const MapSeg sg = segs[s_seg];
     const int local = blockIdx.x - sg.tile_begin;
     const int X0 = (local % sg.tiles_x) * kTile, Y0 = (local / sg.tiles_x) * kTile;
-    const int tid = threadIdx.x;
 
     // Moments are taken of values shifted by a per-tile constant k (the mean of both images
     // at the tile's centre pixel).  The renormalised blur maps constants to themselves, so
-    // blur((a-k)^2) - blur(a-k)^2 equals the reference's blur(a^2) - blur(a)^2 exactly in
-    // real arithmetic, while in FP32 it no longer cancels ~0.25-sized terms down to the
-    // ~1e-5 local variances of smooth regions.  k is symmetric in the two images, so
-    // identical inputs still give bit-identical moments and an SSIM map of exactly 0.
-    __shared__ float s_shift;
+    // blur((a-k)(b-k)) - blur(a-k) blur(b-k) equals the reference's blur(ab) - blur(a)blur(b)
+    // in real arithmetic, while in FP32 it no longer cancels ~0.25-sized terms down to the
+    // ~1e-5 local covariances of smooth regions.  k is symmetric in the two images, so
+    // identical inputs still give bit-identical moments.
     if (tid == 0) {
         const int cx = min(X0 + kTile / 2, sg.w - 1), cy = min(Y0 + kTile / 2, sg.h - 1);
         const int64_t o = (int64_t)cy * sg.pitch + cx;
@@ -267,8 +280,8 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
     // Halo tiles of both images, shifted; zero outside the plane, as the reference's zero
     // padding (src/ssimu2/gaussianblur.hpp:24-36): out-of-image taps add nothing and the
     // renormalisation divides by the in-image tap weights only.
-    for (int i = tid; i < kIn * kIn; i += 256) {
-        const int r = i / kIn, c = i % kIn;
+    for (int i = tid; i < kIn * kIn; i += kMapThreads) {
+        const int r = i / kIn, c = i - r * kIn;
         const int gx = X0 - kHalo + c, gy = Y0 - kHalo + r;
         float va = 0.f, vb = 0.f;
         if (gx >= 0 && gx < sg.w && gy >= 0 && gy < sg.h) {
@@ -281,25 +294,29 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
     }
     __syncthreads();
 
-    // Horizontal pass: 48 rows x 32 columns of the four moment inputs, two adjacent
-    // output columns per work item, divided by the in-bounds tap sum of their column.
-    for (int u = tid; u < kIn * (kTile / 2); u += 256) {
-        const int r = u >> 4, c0 = (u & 15) * 2;
-        float av[18], bv[18], pv[18], qv[18];
+    // Horizontal pass: 48 rows x 32 columns of a-k, b-k, (a-k)(b-k), (a-b)^2; four adjacent
+    // output columns per work item, divided by the in-image tap sum of their column.
+    for (int u = tid; u < kIn * (kTile / 4); u += kMapThreads) {
+        const int r = u >> 3, c0 = (u & 7) * 4;
+        float av[20], bv[20], pv[20], qv[20];
 #pragma unroll
-        for (int j = 0; j < 18; j++) {
+        for (int j = 0; j < 20; j++) {
             av[j] = sa[r][c0 + j];
             bv[j] = sb[r][c0 + j];
             pv[j] = av[j] * bv[j];
             const float dj = av[j] - bv[j];
             qv[j] = dj * dj;
         }
-        float acc[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+        float acc[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int o = 0; o < 4; o++) acc[q][o] = 0.f;
 #pragma unroll
         for (int j = 0; j < 17; j++) {
             const float g = c_gauss[j];
 #pragma unroll
-            for (int o = 0; o < 2; o++) {
+            for (int o = 0; o < 4; o++) {
                 acc[0][o] = fmaf(g, av[j + o], acc[0][o]);
                 acc[1][o] = fmaf(g, bv[j + o], acc[1][o]);
                 acc[2][o] = fmaf(g, pv[j + o], acc[2][o]);
@@ -307,24 +324,24 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
             }
         }
 #pragma unroll
-        for (int o = 0; o < 2; o++) {
-            const float tot = blur_norm(X0 + c0 + o, sg.w);
+        for (int o = 0; o < 4; o++) {
+            const float inv = 1.0f / blur_norm(X0 + c0 + o, sg.w);
 #pragma unroll
-            for (int q = 0; q < 4; q++) sh[q][r][c0 + o] = acc[q][o] / tot;
+            for (int q = 0; q < 4; q++) sh[q][r][c0 + o] = acc[q][o] * inv;
         }
     }
     __syncthreads();
 
-    // Vertical pass: each thread 4 consecutive output rows of one column.
-    const int c = tid & 31, r0 = (tid >> 5) * 4;
-    float mo[4][4];
+    // Vertical pass: each thread 8 consecutive output rows of one column.
+    const int c = tid & 31, r0 = (tid >> 5) * 8;
+    float mo[4][8];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        float col[20];
+        float col[24];
 #pragma unroll
-        for (int j = 0; j < 20; j++) col[j] = sh[q][r0 + j][c];
+        for (int j = 0; j < 24; j++) col[j] = sh[q][r0 + j][c];
 #pragma unroll
-        for (int o = 0; o < 4; o++) {
+        for (int o = 0; o < 8; o++) {
             float acc = 0.f;
 #pragma unroll
             for (int j = 0; j < 17; j++) acc = fmaf(c_gauss[j], col[o + j], acc);
@@ -334,12 +351,12 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
     float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     const int gx = X0 + c;
 #pragma unroll
-    for (int o = 0; o < 4; o++) {
+    for (int o = 0; o < 8; o++) {
         const int gy = Y0 + r0 + o;
         if (gx >= sg.w || gy >= sg.h) continue;
-        const float tot = blur_norm(gy, sg.h);
+        const float inv = 1.0f / blur_norm(gy, sg.h);
         // Shifted means m1 = mu1 - k, m2 = mu2 - k, s12 = blur((a-k)(b-k)), D = blur((a-b)^2).
-        const float m1 = mo[0][o] / tot, m2 = mo[1][o] / tot, s12 = mo[2][o] / tot, D = mo[3][o] / tot;
+        const float m1 = mo[0][o] * inv, m2 = mo[1][o] * inv, s12 = mo[2][o] * inv, D = mo[3][o] * inv;
         // SSIM map of the reference (src/ssimu2/score.hpp:266-274),
         //   ssim = 1 - (1 - md^2) * N / (s1^2 + s2^2 + C),  N = 2 s12' + C,  md = mu1 - mu2,
         // rewritten without cancellation: with V = D - md^2 (the local variance of a - b),
@@ -363,22 +380,22 @@ __global__ void __launch_bounds__(256) ssimu2_maps_kernel(const MapSeg* __restri
     // FP64 tree reduction of the tile.
     double dsum[6];
 #pragma unroll
-    for (int k = 0; k < 6; k++) {
-        double v = (double)sum[k];
+    for (int q = 0; q < 6; q++) {
+        double v = (double)sum[q];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        dsum[k] = v;
+        dsum[q] = v;
     }
     const int warp = tid >> 5, lane = tid & 31;
     if (lane == 0) {
 #pragma unroll
-        for (int k = 0; k < 6; k++) red[warp][k] = dsum[k];
+        for (int q = 0; q < 6; q++) red[warp][q] = dsum[q];
     }
     __syncthreads();
     if (tid < 6) {
         double v = 0.0;
 #pragma unroll
-        for (int w = 0; w < 8; w++) v += red[w][tid];
+        for (int w = 0; w < kMapThreads / 32; w++) v += red[w][tid];
         partials[(int64_t)blockIdx.x * 6 + tid] = v;
     }
 }
@@ -659,7 +676,7 @@ private:
         }
         const int ntiles = tiles_per_pair_ * npairs;
         const int t1 = timer_.begin(1, "ssimu2_maps", st);
-        ssimu2_maps_kernel<<<(unsigned)ntiles, 256, 0, st>>>(segs_d_, segs_per_pair_ * npairs, partials_);
+        ssimu2_maps_kernel<<<(unsigned)ntiles, kMapThreads, 0, st>>>(segs_d_, segs_per_pair_ * npairs, partials_);
         CUDA_CHECK(cudaGetLastError());
         timer_.end(t1, st);
         const int t2 = timer_.begin(2, "ssimu2_final", st);
