@@ -54,6 +54,33 @@ EXPORTPREPROCESS int VshipExt_SSIMU2KernelTimes(Vship_SSIMU2Handler handler, Vsh
 EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliKernelTiming(Vship_ButteraugliHandler handler, int enable);
 EXPORTPREPROCESS int VshipExt_ButteraugliKernelTimes(Vship_ButteraugliHandler handler, VshipExt_KernelTime* out, int max, int reset);
 
+/* Scores one frame pair already in device memory without allocating anything, for callers
+ * that cannot call cudaMalloc: work being recorded into a CUDA graph by stream capture, a
+ * process whose GPU memory is handed out up front by a fixed budget or pool, or a real-time
+ * loop that must never enter the driver's allocator.  This function has no counterpart in the
+ * reference library.
+ *
+ * It runs on the current device, with no handler: the colourspaces are passed directly
+ * (resize and crop are not supported here; use a handler for those).  Inputs are three device
+ * plane pointers per image with byte strides; d_score (device, 1 double) and d_features
+ * (device, 108 floats, may be NULL) receive the results; work is queued on `stream` (NULL is
+ * the legacy default stream) and the call returns without waiting.
+ *
+ * All scratch -- both XYB pyramids, the tile sums and the work list -- lives in a fixed
+ * 32 MiB array inside the library, which every GPU that loads the library holds until the
+ * process exits.  Frames up to 1920x1200 fit; larger frames are rejected with Vship_OutOfVRAM
+ * and a detail giving the bytes needed.  The first call on each device looks up the array's
+ * device address and loads the blur constants (synchronous driver calls), so make that first
+ * call before any stream capture.  Every call shares the one array per device: calls whose
+ * work overlaps on the GPU (different streams, or host threads without ordering) race and
+ * corrupt each other's results; serialise them.  Each call writes every scratch byte it
+ * reads, so nothing left by a previous call leaks into a result. */
+EXPORTPREPROCESS Vship_Exception VshipExt_ComputeSSIMU2NoAlloc(Vship_Colorspace_t src_colorspace,
+                                                                Vship_Colorspace_t dis_colorspace, double* d_score,
+                                                                float* d_features, const uint8_t* const srcp1[3],
+                                                                const uint8_t* const srcp2[3], const int64_t lineSize[3],
+                                                                const int64_t lineSize2[3], void* stream);
+
 /* Metric resolution (after resize and crop) of a handler. */
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2Resolution(Vship_SSIMU2Handler handler, int64_t* width, int64_t* height);
 EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliResolution(Vship_ButteraugliHandler handler, int64_t* width, int64_t* height);

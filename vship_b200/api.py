@@ -68,6 +68,8 @@ def _declare(L):
     L.VshipExt_ButteraugliKernelTimes.argtypes = [HB, c.c_void_p, c.c_int, c.c_int]
     L.VshipExt_ButteraugliKernelTimes.restype = c.c_int
     L.VshipExt_SSIMU2Resolution.argtypes = [H2, i64p, i64p]
+    L.VshipExt_ComputeSSIMU2NoAlloc.argtypes = [abi.Colorspace, abi.Colorspace, c.c_void_p, c.c_void_p, vpp, vpp,
+                                                i64p, i64p, c.c_void_p]
     L.VshipExt_ButteraugliResolution.argtypes = [HB, i64p, i64p]
     return L
 

@@ -292,6 +292,9 @@ int kernel_times(Table<EngineT>& table, unsigned id, VshipExt_KernelTime* out, i
 }
 
 }  // namespace
+
+void record_global_error(const Error& e) { set_global_error(e); }
+
 }  // namespace vship
 
 using namespace vship;

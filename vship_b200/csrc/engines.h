@@ -45,6 +45,7 @@ struct ButterApi {
 };
 
 Ssimu2Api* make_ssimu2_engine();
+void record_global_error(const Error& e);
 ButterApi* make_butter_engine();
 
 }  // namespace vship

@@ -25,12 +25,15 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "colour.cuh"
 #include "frontend.cuh"
 #include "metric_tables.h"
 #include "engines.h"
+#include "../../include/VshipAPI_ext.h"
 
 namespace vship {
 namespace ssimu2 {
@@ -737,8 +740,182 @@ private:
     KernelTimer timer_;
 };
 
+// ------------------------------------------------------------------------------------------
+// Allocation-free scoring (VshipExt_ComputeSSIMU2NoAlloc)
+//
+// Some callers cannot call cudaMalloc: code recording or replaying work inside a stream
+// capture, a process whose GPU memory is handed out up front by a fixed budget or pool, or a
+// real-time loop that must not reach the driver's allocator.  For them this entry point
+// scores one pair already in device memory with the same three kernels as the handler path,
+// but with all of its scratch -- both XYB pyramids, the tile partials and the map work list
+// -- in the file-scope array below.  The array is part of the library image: every GPU that
+// loads the library holds its 32 MiB until the process exits.
+// ------------------------------------------------------------------------------------------
+
+constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 1920x1200 frames fit
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_lock;
+static unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The first call on a device
+// resolves it with cudaGetSymbolAddress (the host-side name is only a stand-in for the
+// device array) and loads the blur constants; later calls reuse the cached address.
+static unsigned char* noalloc_scratch_for_current_device() {
+    int dev = -1;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        VSHIP_THROW(Vship_BadDeviceArgument, "device index beyond the no-allocation table");
+    std::lock_guard<std::mutex> g(g_noalloc_lock);
+    if (g_noalloc_base[dev] == nullptr) {
+        void* ptr = nullptr;
+        CUDA_CHECK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        upload_gauss_constants();
+        g_noalloc_base[dev] = static_cast<unsigned char*>(ptr);
+    }
+    return g_noalloc_base[dev];
+}
+
+// The work list of one pair travels as kernel parameters and is stored into the scratch
+// array on the device, so the entry point issues no copy from host memory.
+struct SegList {
+    MapSeg s[18];
+};
+
+__global__ void noalloc_store_segments_kernel(const __grid_constant__ SegList list, MapSeg* dst, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = list.s[i];
+}
+
+static void compute_no_alloc(const Vship_Colorspace_t& src, const Vship_Colorspace_t& dis, double* d_score,
+                             float* d_features, const uint8_t* const d1[3], const uint8_t* const d2[3],
+                             const int64_t ls1[3], const int64_t ls2[3], cudaStream_t st) {
+    if (!d_score || !d1 || !d2 || !ls1 || !ls2) VSHIP_THROW(Vship_BadPointer, "NULL argument");
+    ClipGeometry geo[2] = {make_geometry(src), make_geometry(dis)};
+    if (geo[0].OW != geo[1].OW || geo[0].OH != geo[1].OH) VSHIP_THROW(Vship_DifferingInputType, "");
+    if (geo[0].generic() || geo[1].generic())
+        VSHIP_THROW(Vship_BadErrorType, "resize and crop need per-handler buffers: use a handler");
+    const Vship_Colorspace_t* cs[2] = {&src, &dis};
+    ColourParams cp[2];
+    for (int c = 0; c < 2; c++) {
+        const int64_t* ls = c ? ls2 : ls1;
+        const uint8_t* const* d = c ? d2 : d1;
+        bool mis = false;
+        for (int p = 0; p < 3; p++) {
+            if (d[p] == nullptr) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
+            if (ls[p] < geo[c].pw[p] * geo[c].bytes) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
+            if (ls[p] % geo[c].bytes) mis = true;
+        }
+        cp[c] = make_colour_params(*cs[c], geo[c], mis);
+    }
+
+    // Pyramid layout, tile count and work list of one pair, as the handler path builds them.
+    Pyramid pyr{};
+    int w = (int)geo[0].OW, h = (int)geo[0].OH;
+    int64_t off = 0;
+    for (int s = 0; s < kScales; s++) {
+        pyr.w[s] = w;
+        pyr.h[s] = h;
+        pyr.pitch[s] = (int)round_up(w, 8);
+        for (int p = 0; p < 3; p++) {
+            if (plane_needed(p, s) || (s == 0 && p == 1)) {
+                pyr.off[s][p] = off;
+                off += round_up((int64_t)pyr.pitch[s] * h, 64);
+            } else {
+                pyr.off[s][p] = -1;
+            }
+        }
+        w = (w - 1) / 2 + 1;
+        h = (h - 1) / 2 + 1;
+    }
+    pyr.image_floats = round_up(off, 64);
+    const size_t xyb_bytes = (size_t)(2 * pyr.image_floats) * sizeof(float);
+    int ntiles = 0, nsegs = 0;
+    for (int s = 0; s < kScales; s++)
+        for (int p = 0; p < 3; p++)
+            if (plane_needed(p, s)) {
+                ntiles += (int)(ceil_div(pyr.w[s], kTile) * ceil_div(pyr.h[s], kTile));
+                nsegs++;
+            }
+    const size_t part_off = round_up((int64_t)xyb_bytes, 256);
+    const size_t seg_off = round_up((int64_t)(part_off + (size_t)ntiles * 6 * sizeof(double)), 256);
+    const size_t need = seg_off + (size_t)nsegs * sizeof(MapSeg);
+    if (need > kNoAllocScratchBytes)
+        VSHIP_THROW(Vship_OutOfVRAM, "frame needs " + std::to_string(need) + " bytes of scratch; the no-allocation entry point has " +
+                                         std::to_string(kNoAllocScratchBytes));
+
+    unsigned char* base = noalloc_scratch_for_current_device();
+    float* xyb = reinterpret_cast<float*>(base);
+    double* partials = reinterpret_cast<double*>(base + part_off);
+    MapSeg* segs_d = reinterpret_cast<MapSeg*>(base + seg_off);
+
+    SegList list{};
+    MapSeg* segs = list.s;
+    int tile = 0, k = 0;
+    for (int s = 0; s < kScales; s++)
+        for (int p = 0; p < 3; p++) {
+            int on = 0;
+            for (int m = 0; m < 3; m++) on |= (map_on(p, s, m) ? 1 : 0) << m;
+            if (!on) continue;
+            MapSeg& g = segs[k++];
+            g = MapSeg{};
+            g.a = xyb + pyr.off[s][p];
+            g.b = xyb + pyr.image_floats + pyr.off[s][p];
+            g.w = pyr.w[s];
+            g.h = pyr.h[s];
+            g.pitch = pyr.pitch[s];
+            g.tiles_x = (int)ceil_div(g.w, kTile);
+            g.ntiles = g.tiles_x * (int)ceil_div(g.h, kTile);
+            g.tile_begin = tile;
+            g.slot = p * 36 + s * 6;
+            g.on = on;
+            tile += g.ntiles;
+        }
+    noalloc_store_segments_kernel<<<1, 32, 0, st>>>(list, segs_d, nsegs);
+    CUDA_CHECK(cudaGetLastError());
+
+    static FrontArgs fa;  // 6.6 KB of kernel arguments, kept off the caller's stack
+    static std::mutex fa_lock;
+    std::lock_guard<std::mutex> g(fa_lock);
+    fa = FrontArgs{};
+    fa.cp[0] = cp[0];
+    fa.cp[1] = cp[1];
+    fa.xyb = xyb;
+    fa.pyr = pyr;
+    for (int c = 0; c < 2; c++)
+        for (int p = 0; p < 3; p++) {
+            fa.raw[c].p[p] = (c ? d2 : d1)[p];
+            fa.raw[c].stride[p] = (c ? ls2 : ls1)[p];
+        }
+    const int smem = (int)sizeof(float) * std::max(chroma_stage_floats(cp[0].subw, cp[0].subh),
+                                                   chroma_stage_floats(cp[1].subw, cp[1].subh));
+    if (smem > 32 * 1024)
+        CUDA_CHECK(cudaFuncSetAttribute(ssimu2_front_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const dim3 fgrid((unsigned)ceil_div(pyr.w[1], 32), (unsigned)ceil_div(pyr.h[1], 32), 2u);
+    ssimu2_front_kernel<false><<<fgrid, 256, smem, st>>>(fa);
+    CUDA_CHECK(cudaGetLastError());
+    ssimu2_maps_kernel<<<(unsigned)ntiles, kMapThreads, 0, st>>>(segs_d, nsegs, partials);
+    CUDA_CHECK(cudaGetLastError());
+    ssimu2_final_kernel<<<1, 256, 0, st>>>(segs_d, nsegs, partials, d_score, d_features);
+    CUDA_CHECK(cudaGetLastError());
+}
+
 }  // namespace ssimu2
 
 Ssimu2Api* make_ssimu2_engine() { return new ssimu2::Engine(); }
 
 }  // namespace vship
+
+extern "C" Vship_Exception VshipExt_ComputeSSIMU2NoAlloc(Vship_Colorspace_t src_colorspace, Vship_Colorspace_t dis_colorspace,
+                                                         double* d_score, float* d_features, const uint8_t* const srcp1[3],
+                                                         const uint8_t* const srcp2[3], const int64_t lineSize[3],
+                                                         const int64_t lineSize2[3], void* stream) {
+    try {
+        vship::ssimu2::compute_no_alloc(src_colorspace, dis_colorspace, d_score, d_features, srcp1, srcp2, lineSize, lineSize2,
+                                        (cudaStream_t)stream);
+    } catch (const vship::Error& e) {
+        vship::record_global_error(e);
+        return e.code;
+    }
+    return Vship_NoError;
+}
