@@ -119,6 +119,26 @@ def make_workload(seed):
     return pairs
 
 
+def pinned_frames(pairs, api, lib=None):
+    """Each frame in one page-locked buffer with its planes back to back, the layout FFVship
+    (the reference's own client) gives Vship_ComputeSSIMU2 (src/ffvship_utility/ffmpegmain.hpp:630-637)."""
+    pinned, host_pairs = [], []
+    for p1, p2, _ in pairs:
+        frames = []
+        for planes in (p1, p2):
+            nbytes = sum(p.nbytes for p in planes)
+            pb = api.PinnedBuffer(nbytes, lib=lib)
+            off, ptrs = 0, []
+            for p in planes:
+                pb.array[off:off + p.nbytes] = p.view(np.uint8).reshape(-1)
+                ptrs.append(pb.ptr.value + off)
+                off += p.nbytes
+            pinned.append(pb)
+            frames.append(ptrs)
+        host_pairs.append((frames[0], frames[1]))
+    return pinned, host_pairs
+
+
 def input_bytes(pairs):
     return sum(p.nbytes for pr in pairs for p in pr[0] + pr[1])
 
@@ -203,16 +223,7 @@ def run_ours(args, world, rank, local):
 
     # ---------------- end to end through the C ABI (e2e) ----------------
     nthreads = args.e2e_threads
-    pinned = []
-    host_pairs = []
-    for p1, p2, _ in pairs:
-        bufs = []
-        for p in list(p1) + list(p2):
-            pb = api.PinnedBuffer(p.nbytes)
-            pb.array[:] = p.view(np.uint8).reshape(-1)
-            pinned.append(pb)
-            bufs.append(pb.ptr.value)
-        host_pairs.append((bufs[:3], bufs[3:]))
+    pinned, host_pairs = pinned_frames(pairs, api)
     handlers = [api.SSIMU2(cs, gpu_id=local) for _ in range(nthreads)]
     e2e_scores = np.zeros(BATCH)
 
@@ -267,7 +278,8 @@ def run_ours(args, world, rank, local):
         "config": {"workload": WORKLOAD, "pairs_per_step": BATCH, "width": W, "height": H,
                    "format": "YUV420 10-bit limited BT.709", "parallelism": "replicas" if world > 1 else "single",
                    "l2": "inputs (%.0f MB per step) larger than L2" % (input_bytes(pairs) / 1e6)},
-        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "api": "Vship_ComputeSSIMU2 (pinned host buffers)",
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
+                "api": "Vship_ComputeSSIMU2, each frame in one pinned buffer (FFVship layout)",
                 "threads_handlers": nthreads, "timer": "wall clock, synchronised",
                 "h2d_bytes_per_step": input_bytes(pairs), "d2h_bytes_per_step": BATCH * (8 + 108 * 4),
                 "max_abs_score_diff_vs_device_path": max_dev},
@@ -313,15 +325,7 @@ def run_reference(args, world, rank, local):
     cs = abi.yuv420_10bit_bt709(W, H)
     pairs = make_workload(seed=1234)
     ls = pairs[0][2]
-    pinned, host_pairs = [], []
-    for p1, p2, _ in pairs:
-        bufs = []
-        for p in list(p1) + list(p2):
-            pb = api.PinnedBuffer(p.nbytes, lib=L)
-            pb.array[:] = p.view(np.uint8).reshape(-1)
-            pinned.append(pb)
-            bufs.append(pb.ptr.value)
-        host_pairs.append((bufs[:3], bufs[3:]))
+    pinned, host_pairs = pinned_frames(pairs, api, lib=L)
     best = None
     for nthreads in args.ref_threads:
         handlers = [api.SSIMU2(cs, gpu_id=local, lib=L) for _ in range(nthreads)]
@@ -363,7 +367,8 @@ def run_reference(args, world, rank, local):
         "config": {"workload": WORKLOAD, "pairs_per_step": BATCH, "width": W, "height": H,
                    "format": "YUV420 10-bit limited BT.709",
                    "library": "Vship 4.1.0 built from its sources with nvcc for sm_100a (oracle/build_ref.sh)",
-                   "api": "Vship_ComputeSSIMU2 with pinned host buffers", "threads_handlers": nthreads,
+                   "api": "Vship_ComputeSSIMU2, each frame in one pinned buffer (FFVship layout)",
+                   "threads_handlers": nthreads,
                    "threads_swept": args.ref_threads},
         "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "kind": "reference", "cores": nthreads,
@@ -371,6 +376,28 @@ def run_reference(args, world, rank, local):
                                    "build runs on the B200, driven by %d host threads" % (args.steps, BATCH, nthreads)},
     }
     print(json.dumps(line), flush=True)
+
+
+def run_profile_case(args):
+    """Small device-resident run for ncu captures: `--profile-pairs` 1080p pairs, `--steps`
+    calls of VshipExt_ComputeSSIMU2Device, nothing else (no timing, no e2e, no CPU leg)."""
+    import torch
+    from vship_b200 import abi, api, synth
+    n = args.profile_pairs
+    pairs = synth.make_pairs(n, W, H, fmt="yuv420p10", seed=5, unique=2)
+    cs = abi.yuv420_10bit_bt709(W, H)
+    ls = pairs[0][2]
+    dev = [([torch.from_numpy(p.view(np.uint8)).cuda() for p in a], [torch.from_numpy(p.view(np.uint8)).cuda() for p in b])
+           for a, b, _ in pairs]
+    ptr1 = [t.data_ptr() for d in dev for t in d[0]]
+    ptr2 = [t.data_ptr() for d in dev for t in d[1]]
+    scores = torch.zeros(n, dtype=torch.float64, device="cuda")
+    h = api.SSIMU2(cs)
+    for _ in range(args.steps):
+        h.compute_device(n, ptr1, ptr2, ls, ls, scores.data_ptr(), 0, 0)
+    torch.cuda.synchronize()
+    h.close()
+    log("profile case: %d pairs x %d calls, scores %s" % (n, args.steps, np.round(scores.cpu().numpy()[:4], 4)))
 
 
 def main():
@@ -383,7 +410,12 @@ def main():
     ap.add_argument("--ref-threads", type=int, nargs="+", default=[1, 3, 4, 8])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-pairs", type=int, default=0,
+                    help="only run N device-resident pairs --steps times (for ncu captures)")
     args = ap.parse_args()
+    if args.profile_pairs:
+        run_profile_case(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_env()

@@ -106,3 +106,32 @@ def test_errors(gpu):
             h.compute(p, p, [32, 64, 64])
         assert e.value.code == abi.BadPointer
         assert h.compute(p, p, [64] * 3) == 100.0
+
+
+def test_contiguous_frame_single_copy_matches_separate_planes(gpu):
+    # FFVship lays a frame's planes back to back in one pinned buffer; the engine then copies
+    # the frame in one transfer and reads it with the caller's strides.
+    w, h = 333, 201
+    p1, p2, ls = synth.make_pairs(1, w, h, fmt="yuv420p10", seed=17)[0]
+    cs = abi.yuv420_10bit_bt709(w, h)
+    with api.SSIMU2(cs) as hd:
+        separate = hd.compute(p1, p2, ls)
+        for pad in ([0, 0, 0], [6, 2, 10], [3, 1, 5]):   # the last one gives odd strides
+            f1, pls = synth.with_padding(p1, ls, pad)
+            f2, _ = synth.with_padding(p2, ls, pad)
+            buf1 = np.concatenate([f.reshape(-1) for f in f1])
+            buf2 = np.concatenate([f.reshape(-1) for f in f2])
+            o = np.cumsum([0] + [f.nbytes for f in f1])
+            ptr1 = [buf1.ctypes.data + int(o[i]) for i in range(3)]
+            ptr2 = [buf2.ctypes.data + int(o[i]) for i in range(3)]
+            assert hd.compute(ptr1, ptr2, pls) == separate
+    with api.Butteraugli(cs, qnorm=5) as hb:
+        sep, _ = hb.compute(p1, p2, ls)
+        f1, pls = synth.with_padding(p1, ls, [6, 2, 10])
+        f2, _ = synth.with_padding(p2, ls, [6, 2, 10])
+        buf1 = np.concatenate([f.reshape(-1) for f in f1])
+        buf2 = np.concatenate([f.reshape(-1) for f in f2])
+        o = np.cumsum([0] + [f.nbytes for f in f1])
+        got, _ = hb.compute([buf1.ctypes.data + int(o[i]) for i in range(3)],
+                            [buf2.ctypes.data + int(o[i]) for i in range(3)], pls)
+        assert got == sep

@@ -672,8 +672,8 @@ public:
         CUDA_CHECK(cudaEventCreateWithFlags(&last_done_, cudaEventDisableTiming));
         upload_constants();
         for (int c = 0; c < 2; c++) {
-            staged_bytes_[c] = dense_image_bytes(geo_[c], staged_off_[c]);
-            staged_[c] = device_alloc<uint8_t>((size_t)staged_bytes_[c], "input staging");
+            int64_t off[3];
+            staging_[c].ensure((size_t)dense_image_bytes(geo_[c], off), stream_);
             if (generic_) lin_generic_[c].alloc(geo_[c]);
         }
         const int64_t n0 = (int64_t)w_ * h_;
@@ -690,21 +690,19 @@ public:
     void compute(double norms[3], uint8_t* dstp, int64_t dststride, const uint8_t* const s1[3], const uint8_t* const s2[3],
                  const int64_t ls1[3], const int64_t ls2[3]) override {
         CUDA_CHECK(cudaStreamWaitEvent(stream_, last_done_, 0));
-        stage_host_image(staged_[0], staged_off_[0], geo_[0], s1, ls1, stream_);
-        stage_host_image(staged_[1], staged_off_[1], geo_[1], s2, ls2, stream_);
         RawImage raw[2];
-        for (int c = 0; c < 2; c++)
-            for (int p = 0; p < 3; p++) {
-                raw[c].p[p] = staged_[c] + staged_off_[c][p];
-                raw[c].stride[p] = geo_[c].pw[p] * geo_[c].bytes;
-            }
+        ColourParams cp[2] = {cp_[0], cp_[1]};
+        for (int c = 0; c < 2; c++) {
+            raw[c] = stage_host_image(staging_[c], geo_[c], c ? s2 : s1, c ? ls2 : ls1, stream_);
+            cp[c].misaligned = misaligned_view(raw[c], geo_[c]) ? 1 : 0;
+        }
         float* dmap = nullptr;
         if (dstp) {
             if (dststride < (int64_t)w_ * 4) VSHIP_THROW(Vship_BadPointer, "dststride smaller than width * 4");
             ensure_distmap();
             dmap = distmap_d_;
         }
-        run(raw, cp_, stream_, norms_d_, dmap, w_);
+        run(raw, cp, stream_, norms_d_, dmap, w_);
         CUDA_CHECK(cudaMemcpyAsync(norms_host_, norms_d_, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
         if (dstp)
             CUDA_CHECK(cudaMemcpy2DAsync(dstp, (size_t)dststride, distmap_d_, (size_t)w_ * 4, (size_t)w_ * 4, (size_t)h_,
@@ -850,8 +848,7 @@ private:
         if (stream_) (void)cudaStreamSynchronize(stream_);
         timer_.destroy();
         for (int c = 0; c < 2; c++) {
-            device_free(staged_[c]);
-            staged_[c] = nullptr;
+            staging_[c].free();
             lin_generic_[c].free();
         }
         device_free(pool_);
@@ -878,9 +875,7 @@ private:
     int w_ = 0, h_ = 0, qnorm_ = 2;
     float intensity_ = 203.f;
     cudaStream_t stream_ = nullptr;
-    uint8_t* staged_[2] = {nullptr, nullptr};
-    int64_t staged_off_[2][3] = {};
-    int64_t staged_bytes_[2] = {0, 0};
+    StagingBuffer staging_[2];
     GenericLinear lin_generic_[2];
     int64_t plane_floats_ = 0;
     float* pool_ = nullptr;

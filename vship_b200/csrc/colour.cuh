@@ -435,4 +435,60 @@ __device__ __forceinline__ float3 ingest_pixel(const RawImage& im, int64_t X, in
     return to_linear_709(v, cp);
 }
 
+// ---------------------------------------------------------------------------------------
+// Compile-time specialised pixel paths for the two most common clip formats; every other
+// colourspace takes the generic runtime-dispatched path above.  Results are identical to the
+// generic path (same operations in the same order), only the dispatch is resolved at compile
+// time.
+//   kFastYuv420Bt709: 16-bit containers, 4:2:0, Left siting, BT.709 matrix, transfer, primaries
+//   kFastRgb8Srgb:    8-bit R'G'B' 4:4:4, sRGB transfer, BT.709 primaries
+// ---------------------------------------------------------------------------------------
+constexpr int kFastGeneric = 0, kFastYuv420Bt709 = 1, kFastRgb8Srgb = 2;
+
+__host__ __device__ inline int fast_path_of(const ColourParams& cp) {
+    const bool u16 = cp.sample != Vship_SampleUINT8 && cp.sample != Vship_SampleFLOAT && cp.sample != Vship_SampleHALF;
+    if (u16 && !cp.misaligned && cp.subw == 1 && cp.subh == 1 && !cp.hcenter && cp.vcenter && cp.yuv_chroma &&
+        cp.matrix == Vship_MATRIX_BT709 && cp.trc == Vship_TRC_BT709 && cp.primaries == Vship_PRIMARIES_BT709)
+        return kFastYuv420Bt709;
+    if (cp.sample == Vship_SampleUINT8 && cp.subw == 0 && cp.subh == 0 && !cp.yuv_chroma && cp.matrix == Vship_MATRIX_RGB &&
+        cp.trc == Vship_TRC_sRGB && cp.primaries == Vship_PRIMARIES_BT709)
+        return kFastRgb8Srgb;
+    return kFastGeneric;
+}
+
+__device__ __forceinline__ float srgb_to_linear(float a) {
+    if (a < 0) return a < -0.04045f ? -fast_pow((-a + 0.055f) * (1.0f / 1.055f), 2.4f) : a * (1.0f / 12.92f);
+    return a > 0.04045f ? fast_pow((a + 0.055f) * (1.0f / 1.055f), 2.4f) : a * (1.0f / 12.92f);
+}
+
+__device__ __forceinline__ float range_luma(float v, const ColourParams& cp) {
+    if (cp.full_range) return v * cp.full_scale;
+    return (v * cp.lim_scale - 16.f) * (1.0f / 219.f);
+}
+
+template <int kFast>
+__device__ __forceinline__ float3 ingest_fast(const RawImage& im, const ColourParams& cp, const ChromaStage& st, int X, int Y,
+                                             int X0, int Y0) {
+    if constexpr (kFast == kFastYuv420Bt709) {
+        const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(im.p[0] + (int64_t)Y * im.stride[0]) + X);
+        float3 v;
+        v.x = range_luma((float)(u & cp.mask), cp);
+        const float2 c = chroma_from_stage(st, cp, X - X0, Y - Y0);
+        v.y = c.x;
+        v.z = c.y;
+        v = ncl_to_rgb(v, 0.2126f, 0.0722f);
+        v.x = signed_powf(v.x, 2.4f);
+        v.y = signed_powf(v.y, 2.4f);
+        v.z = signed_powf(v.z, 2.4f);
+        return v;
+    } else {
+        const int64_t o = (int64_t)Y * im.stride[0] + X;
+        float3 v;
+        v.x = srgb_to_linear(range_luma((float)__ldg(im.p[0] + o), cp));
+        v.y = srgb_to_linear(range_luma((float)__ldg(im.p[1] + (int64_t)Y * im.stride[1] + X), cp));
+        v.z = srgb_to_linear(range_luma((float)__ldg(im.p[2] + (int64_t)Y * im.stride[2] + X), cp));
+        return v;
+    }
+}
+
 }  // namespace vship

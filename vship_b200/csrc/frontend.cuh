@@ -113,20 +113,73 @@ inline int64_t dense_image_bytes(const ClipGeometry& g, int64_t plane_off[3]) {
     return off;
 }
 
-// Copies three host planes with arbitrary byte strides into a dense device image.
-inline void stage_host_image(uint8_t* dst, const int64_t plane_off[3], const ClipGeometry& g,
-                             const uint8_t* const src[3], const int64_t line_size[3], cudaStream_t stream) {
+// Device staging area of one input image; grows (never shrinks) when a caller's strides need
+// more room than the dense layout allocated at Init.
+struct StagingBuffer {
+    uint8_t* ptr = nullptr;
+    size_t cap = 0;
+    void ensure(size_t n, cudaStream_t stream) {
+        if (n <= cap) return;
+        CUDA_CHECK(cudaStreamSynchronize(stream));
+        device_free(ptr);
+        ptr = nullptr;
+        cap = 0;
+        ptr = device_alloc<uint8_t>(n, "input staging");
+        cap = n;
+    }
+    void free() {
+        device_free(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+};
+
+// Copies the three host planes of one image to the device and returns the device view.
+// When the planes lie back to back in one host allocation (as FFVship lays out its pinned
+// frames), the whole frame goes in one copy and keeps the caller's strides; otherwise each
+// plane is copied densely.  Bytes past the last row of the last plane are never read (the
+// copy size follows src/gpuColorToLinear/vshipColor.hpp:96).
+inline RawImage stage_host_image(StagingBuffer& buf, const ClipGeometry& g, const uint8_t* const src[3],
+                                 const int64_t line_size[3], cudaStream_t stream) {
+    int64_t row[3];
     for (int c = 0; c < 3; c++) {
         if (src[c] == nullptr) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
-        const int64_t row = g.pw[c] * g.bytes;
-        if (line_size[c] < row) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
-        if (line_size[c] == row) {
-            CUDA_CHECK(cudaMemcpyAsync(dst + plane_off[c], src[c], (size_t)(row * g.ph[c]), cudaMemcpyHostToDevice, stream));
+        row[c] = g.pw[c] * g.bytes;
+        if (line_size[c] < row[c]) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
+    }
+    RawImage im;
+    const bool contiguous = src[1] == src[0] + line_size[0] * g.ph[0] && src[2] == src[1] + line_size[1] * g.ph[1];
+    if (contiguous) {
+        const int64_t bytes = line_size[0] * g.ph[0] + line_size[1] * g.ph[1] + line_size[2] * (g.ph[2] - 1) + row[2];
+        buf.ensure((size_t)round_up(bytes, 256), stream);
+        CUDA_CHECK(cudaMemcpyAsync(buf.ptr, src[0], (size_t)bytes, cudaMemcpyHostToDevice, stream));
+        for (int c = 0; c < 3; c++) {
+            im.p[c] = buf.ptr + (src[c] - src[0]);
+            im.stride[c] = line_size[c];
+        }
+        return im;
+    }
+    int64_t off[3];
+    const int64_t total = dense_image_bytes(g, off);
+    buf.ensure((size_t)total, stream);
+    for (int c = 0; c < 3; c++) {
+        im.p[c] = buf.ptr + off[c];
+        im.stride[c] = row[c];
+        if (line_size[c] == row[c]) {
+            CUDA_CHECK(cudaMemcpyAsync(buf.ptr + off[c], src[c], (size_t)(row[c] * g.ph[c]), cudaMemcpyHostToDevice, stream));
         } else {
-            CUDA_CHECK(cudaMemcpy2DAsync(dst + plane_off[c], (size_t)row, src[c], (size_t)line_size[c], (size_t)row,
+            CUDA_CHECK(cudaMemcpy2DAsync(buf.ptr + off[c], (size_t)row[c], src[c], (size_t)line_size[c], (size_t)row[c],
                                          (size_t)g.ph[c], cudaMemcpyHostToDevice, stream));
         }
     }
+    return im;
+}
+
+// A stride that is not a multiple of the sample size makes the kernels use byte loads.
+inline bool misaligned_view(const RawImage& im, const ClipGeometry& g) {
+    for (int c = 0; c < 3; c++)
+        if (im.stride[c] % g.bytes || (reinterpret_cast<uintptr_t>(im.p[c]) % g.bytes)) return true;
+    return false;
 }
 
 // ---- generic path: ingest to planar linear RGB, then resize (horizontalResizeTranspose,

@@ -144,7 +144,7 @@ __device__ __forceinline__ void build_level(const LevelTile<2 * T>& src, LevelTi
     }
 }
 
-template <bool FromLinear>
+template <bool FromLinear, int kFast>
 __global__ void __launch_bounds__(256) ssimu2_front_kernel(const __grid_constant__ FrontArgs a) {
     __shared__ LevelTile<32> t1;
     __shared__ LevelTile<16> t2;
@@ -161,14 +161,17 @@ __global__ void __launch_bounds__(256) ssimu2_front_kernel(const __grid_constant
     const RawImage& im = a.raw[img];
     extern __shared__ float stage_mem[];
     ChromaStage st{};
-    if (!FromLinear && (cp.subw || cp.subh)) chroma_stage(im, cp, blockIdx.x * kStageTile, blockIdx.y * kStageTile, stage_mem, st);
+    if (!FromLinear && kFast != kFastRgb8Srgb && (cp.subw || cp.subh))
+        chroma_stage(im, cp, blockIdx.x * kStageTile, blockIdx.y * kStageTile, stage_mem, st);
 
     auto pixel = [&](int X, int Y) -> float3 {
         if (FromLinear) {
             const float* base = a.lin[clip] + (int64_t)Y * a.lin_pitch[clip] + X;
             return make_float3(base[0], base[a.lin_plane[clip]], base[2 * a.lin_plane[clip]]);
-        } else {
+        } else if (kFast == kFastGeneric) {
             return ingest_staged(im, cp, st, X, Y, blockIdx.x * kStageTile, blockIdx.y * kStageTile);
+        } else {
+            return ingest_fast<kFast>(im, cp, st, X, Y, blockIdx.x * kStageTile, blockIdx.y * kStageTile);
         }
     };
 
@@ -242,164 +245,232 @@ __device__ __forceinline__ float blur_norm(int pos, int n) {
 
 constexpr int kMapThreads = 128;
 
-__global__ void __launch_bounds__(kMapThreads) ssimu2_maps_kernel(const MapSeg* __restrict__ segs, int nseg,
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+
+// Packed FP32x2 multiply-add of sm_100: one issue slot for two independent FMAs.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// The work list of one pair, passed by value: the pairs of a batch differ only in their base
+// pointer (pair p's reference plane is xyb + 2p * image_floats + off, its distorted plane
+// image_floats further).
+struct MapTemplate {
+    struct Seg {
+        int64_t off;
+        int w, h, pitch, tiles_x, tile_begin;
+    } seg[18];
+    int nseg;
+    int tiles_per_pair;
+    const float* xyb;
+    int64_t image_floats;
+};
+
+constexpr int kHaloPerThread = kIn * kIn / kMapThreads;  // 18
+static_assert(kIn * kIn % kMapThreads == 0, "halo tile must split evenly over the threads");
+
+struct TileRef {
+    const float* a;
+    const float* b;
+    int w, h, pitch, X0, Y0;
+};
+
+__device__ __forceinline__ TileRef locate_tile(const MapTemplate& mt, int tile) {
+    const int pair = tile / mt.tiles_per_pair;
+    const int lt = tile - pair * mt.tiles_per_pair;
+    int s = 0;
+#pragma unroll 1
+    for (int i = 1; i < mt.nseg; i++)
+        if (mt.seg[i].tile_begin <= lt) s = i;
+    const MapTemplate::Seg& g = mt.seg[s];
+    TileRef t;
+    t.a = mt.xyb + (int64_t)(2 * pair) * mt.image_floats + g.off;
+    t.b = t.a + mt.image_floats;
+    t.w = g.w;
+    t.h = g.h;
+    t.pitch = g.pitch;
+    const int l = lt - g.tile_begin;
+    const int ty = l / g.tiles_x;
+    t.X0 = (l - ty * g.tiles_x) * kTile;
+    t.Y0 = ty * kTile;
+    return t;
+}
+
+// Issues the loads of a tile's 48x48 halo of both images into registers (element
+// i = tid + 128 * it of the row-major halo); out-of-image elements read as 0.
+__device__ __forceinline__ void load_halo(const TileRef& t, float (&ra)[kHaloPerThread], float (&rb)[kHaloPerThread],
+                                          unsigned& inmask) {
+    inmask = 0;
+#pragma unroll
+    for (int it = 0; it < kHaloPerThread; it++) {
+        const int i = threadIdx.x + it * kMapThreads;
+        const int r = i / kIn, c = i - r * kIn;
+        const int gx = t.X0 - kHalo + c, gy = t.Y0 - kHalo + r;
+        const bool in = gx >= 0 && gx < t.w && gy >= 0 && gy < t.h;
+        const int64_t o = in ? (int64_t)gy * t.pitch + gx : 0;
+        ra[it] = in ? __ldg(t.a + o) : 0.f;
+        rb[it] = in ? __ldg(t.b + o) : 0.f;
+        inmask |= (in ? 1u : 0u) << it;
+    }
+}
+
+// Persistent: CTA b scores tiles b, b + gridDim.x, ...; the halo of the next tile is loaded
+// into registers while the current one is blurred.
+__global__ void __launch_bounds__(kMapThreads) ssimu2_maps_kernel(const __grid_constant__ MapTemplate mt, int total_tiles,
                                                                   double* __restrict__ partials) {
-    __shared__ float sa[kIn][kIn + 1];
-    __shared__ float sb[kIn][kIn + 1];
-    __shared__ float sh[4][kIn][kTile + 1];
+    // Moment inputs are kept as float2 pairs so one 64-bit shared access and one packed FMA
+    // serve two quantities: (a-k, b-k) and ((a-k)(b-k), (a-b)^2).
+    __shared__ float2 sab[kIn][kIn + 1];
+    __shared__ float2 hab[kIn][kTile + 1];
+    __shared__ float2 hpq[kIn][kTile + 1];
     __shared__ double red[kMapThreads / 32][6];
-    __shared__ int s_seg;
     __shared__ float s_shift;
 
     const int tid = threadIdx.x;
-    if (tid == 0) {
-        int lo = 0, hi = nseg - 1;
-        const int t = blockIdx.x;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (segs[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
-        }
-        s_seg = lo;
-    }
-    __syncthreads();
-    const MapSeg sg = segs[s_seg];
-    const int local = blockIdx.x - sg.tile_begin;
-    const int X0 = (local % sg.tiles_x) * kTile, Y0 = (local / sg.tiles_x) * kTile;
+    int tile = blockIdx.x;
+    if (tile >= total_tiles) return;
+    TileRef cur = locate_tile(mt, tile);
+    float ra[kHaloPerThread], rb[kHaloPerThread];
+    unsigned inmask;
+    load_halo(cur, ra, rb, inmask);
 
-    // Moments are taken of values shifted by a per-tile constant k (the mean of both images
-    // at the tile's centre pixel).  The renormalised blur maps constants to themselves, so
-    // blur((a-k)(b-k)) - blur(a-k) blur(b-k) equals the reference's blur(ab) - blur(a)blur(b)
-    // in real arithmetic, while in FP32 it no longer cancels ~0.25-sized terms down to the
-    // ~1e-5 local covariances of smooth regions.  k is symmetric in the two images, so
-    // identical inputs still give bit-identical moments.
-    if (tid == 0) {
-        const int cx = min(X0 + kTile / 2, sg.w - 1), cy = min(Y0 + kTile / 2, sg.h - 1);
-        const int64_t o = (int64_t)cy * sg.pitch + cx;
-        s_shift = 0.5f * (__ldg(sg.a + o) + __ldg(sg.b + o));
-    }
-    __syncthreads();
-    const float k = s_shift;
-
-    // Halo tiles of both images, shifted; zero outside the plane, as the reference's zero
-    // padding (src/ssimu2/gaussianblur.hpp:24-36): out-of-image taps add nothing and the
-    // renormalisation divides by the in-image tap weights only.
-    for (int i = tid; i < kIn * kIn; i += kMapThreads) {
-        const int r = i / kIn, c = i - r * kIn;
-        const int gx = X0 - kHalo + c, gy = Y0 - kHalo + r;
-        float va = 0.f, vb = 0.f;
-        if (gx >= 0 && gx < sg.w && gy >= 0 && gy < sg.h) {
-            const int64_t o = (int64_t)gy * sg.pitch + gx;
-            va = __ldg(sg.a + o) - k;
-            vb = __ldg(sg.b + o) - k;
+    while (true) {
+        // Shift constant k: the mean of both images at the tile's first output pixel (halo
+        // element (8, 8), held by thread 8 as its 4th element; always inside the image).
+        // The renormalised blur maps constants to themselves, so moments of a-k, b-k give the
+        // reference's blur(ab) - blur(a)blur(b) etc. in exact arithmetic, while in FP32 they
+        // no longer cancel ~0.25-sized terms down to the ~1e-5 local covariances of smooth
+        // regions.  k is symmetric in the two images, so identical inputs still give
+        // bit-identical moments.
+        static_assert(kHalo * kIn + kHalo == 8 + 3 * kMapThreads, "shift element owner");
+        if (tid == 8) s_shift = 0.5f * (ra[3] + rb[3]);
+        __syncthreads();
+        const float k = s_shift;
+        // Shifted halo; zero outside the plane, as the reference's zero padding
+        // (src/ssimu2/gaussianblur.hpp:24-36): out-of-image taps add nothing and the
+        // renormalisation divides by the in-image tap weights only.
+#pragma unroll
+        for (int it = 0; it < kHaloPerThread; it++) {
+            const int i = tid + it * kMapThreads;
+            const int r = i / kIn, c = i - r * kIn;
+            const bool in = (inmask >> it) & 1u;
+            sab[r][c] = in ? f2(ra[it] - k, rb[it] - k) : f2(0.f, 0.f);
         }
-        sa[r][c] = va;
-        sb[r][c] = vb;
-    }
-    __syncthreads();
-
-    // Horizontal pass: 48 rows x 32 columns of a-k, b-k, (a-k)(b-k), (a-b)^2; four adjacent
-    // output columns per work item, divided by the in-image tap sum of their column.
-    for (int u = tid; u < kIn * (kTile / 4); u += kMapThreads) {
-        const int r = u >> 3, c0 = (u & 7) * 4;
-        float av[20], bv[20], pv[20], qv[20];
-#pragma unroll
-        for (int j = 0; j < 20; j++) {
-            av[j] = sa[r][c0 + j];
-            bv[j] = sb[r][c0 + j];
-            pv[j] = av[j] * bv[j];
-            const float dj = av[j] - bv[j];
-            qv[j] = dj * dj;
+        __syncthreads();
+        const int X0 = cur.X0, Y0 = cur.Y0, w = cur.w, h = cur.h;
+        const int next = tile + gridDim.x;
+        if (next < total_tiles) {
+            cur = locate_tile(mt, next);
+            load_halo(cur, ra, rb, inmask);
         }
-        float acc[4][4];
+
+        // Horizontal pass: 48 rows x 32 columns; a work item is four adjacent output columns
+        // of one row; consecutive threads take consecutive rows (conflict-free 64-bit access).
+        for (int u = tid; u < kIn * (kTile / 4); u += kMapThreads) {
+            const int cg = u / kIn, r = u - cg * kIn, c0 = cg * 4;
+            float2 ab[20], pq[20];
 #pragma unroll
-        for (int q = 0; q < 4; q++)
+            for (int j = 0; j < 20; j++) {
+                ab[j] = sab[r][c0 + j];
+                const float d = ab[j].x - ab[j].y;
+                pq[j] = f2(ab[j].x * ab[j].y, d * d);
+            }
+            float2 acc_ab[4], acc_pq[4];
 #pragma unroll
-            for (int o = 0; o < 4; o++) acc[q][o] = 0.f;
+            for (int o = 0; o < 4; o++) acc_ab[o] = acc_pq[o] = f2(0.f, 0.f);
 #pragma unroll
-        for (int j = 0; j < 17; j++) {
-            const float g = c_gauss[j];
+            for (int j = 0; j < 17; j++) {
+                const float2 g = f2(c_gauss[j], c_gauss[j]);
+#pragma unroll
+                for (int o = 0; o < 4; o++) {
+                    acc_ab[o] = fma2(g, ab[j + o], acc_ab[o]);
+                    acc_pq[o] = fma2(g, pq[j + o], acc_pq[o]);
+                }
+            }
 #pragma unroll
             for (int o = 0; o < 4; o++) {
-                acc[0][o] = fmaf(g, av[j + o], acc[0][o]);
-                acc[1][o] = fmaf(g, bv[j + o], acc[1][o]);
-                acc[2][o] = fmaf(g, pv[j + o], acc[2][o]);
-                acc[3][o] = fmaf(g, qv[j + o], acc[3][o]);
+                const float inv = 1.0f / blur_norm(X0 + c0 + o, w);
+                hab[r][c0 + o] = f2(acc_ab[o].x * inv, acc_ab[o].y * inv);
+                hpq[r][c0 + o] = f2(acc_pq[o].x * inv, acc_pq[o].y * inv);
             }
         }
-#pragma unroll
-        for (int o = 0; o < 4; o++) {
-            const float inv = 1.0f / blur_norm(X0 + c0 + o, sg.w);
-#pragma unroll
-            for (int q = 0; q < 4; q++) sh[q][r][c0 + o] = acc[q][o] * inv;
-        }
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // Vertical pass: each thread 8 consecutive output rows of one column.
-    const int c = tid & 31, r0 = (tid >> 5) * 8;
-    float mo[4][8];
+        // Vertical pass: each thread 8 consecutive output rows of one column.
+        const int c = tid & 31, r0 = (tid >> 5) * 8;
+        float2 mab[8], mpq[8];
+        {
+            float2 col[24];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        float col[24];
+            for (int j = 0; j < 24; j++) col[j] = hab[r0 + j][c];
 #pragma unroll
-        for (int j = 0; j < 24; j++) col[j] = sh[q][r0 + j][c];
+            for (int o = 0; o < 8; o++) {
+                float2 acc = f2(0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 17; j++) acc = fma2(f2(c_gauss[j], c_gauss[j]), col[o + j], acc);
+                mab[o] = acc;
+            }
+#pragma unroll
+            for (int j = 0; j < 24; j++) col[j] = hpq[r0 + j][c];
+#pragma unroll
+            for (int o = 0; o < 8; o++) {
+                float2 acc = f2(0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 17; j++) acc = fma2(f2(c_gauss[j], c_gauss[j]), col[o + j], acc);
+                mpq[o] = acc;
+            }
+        }
+        float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const int gx = X0 + c;
 #pragma unroll
         for (int o = 0; o < 8; o++) {
-            float acc = 0.f;
-#pragma unroll
-            for (int j = 0; j < 17; j++) acc = fmaf(c_gauss[j], col[o + j], acc);
-            mo[q][o] = acc;
+            const int gy = Y0 + r0 + o;
+            if (gx >= w || gy >= h) continue;
+            const float inv = 1.0f / blur_norm(gy, h);
+            // Shifted means m1 = mu1 - k, m2 = mu2 - k, s12 = blur((a-k)(b-k)), D = blur((a-b)^2).
+            const float m1 = mab[o].x * inv, m2 = mab[o].y * inv, s12 = mpq[o].x * inv, D = mpq[o].y * inv;
+            // SSIM map of the reference (src/ssimu2/score.hpp:266-274),
+            //   ssim = 1 - (1 - md^2) * N / (s1^2 + s2^2 + C),  N = 2 s12' + C,  md = mu1 - mu2,
+            // rewritten without cancellation: with V = D - md^2 (the local variance of a - b),
+            // s1^2 + s2^2 + C = V + N and therefore ssim = (V + md^2 N) / (V + N).  Identical
+            // inputs give V = md = 0 and an SSIM of exactly 0.
+            const float md = m1 - m2;
+            const float md2 = md * md;
+            const float N = fmaf(2.0f, s12 - m1 * m2, 0.0009f);
+            const float V = D - md2;
+            const float ssim = fmaxf(fmaf(md2, N, V) / (V + N), 0.0f);
+            // Artifact and detail-loss maps (score.hpp:276-281): (|b-mu2|+1)/(|a-mu1|+1) - 1,
+            // evaluated as (|b-mu2| - |a-mu1|) / (|a-mu1| + 1) to avoid cancelling against 1.
+            const float2 cv = sab[r0 + o + kHalo][c + kHalo];
+            const float ea = fabsf(cv.x - m1), eb = fabsf(cv.y - m2);
+            const float v1 = (eb - ea) / (ea + 1.0f);
+            const float art = fmaxf(v1, 0.0f), det = fmaxf(-v1, 0.0f);
+            const float s2 = ssim * ssim, a2 = art * art, d2 = det * det;
+            sum[0] += ssim; sum[1] += art; sum[2] += det;
+            sum[3] += s2 * s2; sum[4] += a2 * a2; sum[5] += d2 * d2;
         }
-    }
-    float sum[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const int gx = X0 + c;
+        // FP64 tree reduction of the tile.
+        double dsum[6];
 #pragma unroll
-    for (int o = 0; o < 8; o++) {
-        const int gy = Y0 + r0 + o;
-        if (gx >= sg.w || gy >= sg.h) continue;
-        const float inv = 1.0f / blur_norm(gy, sg.h);
-        // Shifted means m1 = mu1 - k, m2 = mu2 - k, s12 = blur((a-k)(b-k)), D = blur((a-b)^2).
-        const float m1 = mo[0][o] * inv, m2 = mo[1][o] * inv, s12 = mo[2][o] * inv, D = mo[3][o] * inv;
-        // SSIM map of the reference (src/ssimu2/score.hpp:266-274),
-        //   ssim = 1 - (1 - md^2) * N / (s1^2 + s2^2 + C),  N = 2 s12' + C,  md = mu1 - mu2,
-        // rewritten without cancellation: with V = D - md^2 (the local variance of a - b),
-        // s1^2 + s2^2 + C = V + N and therefore ssim = (V + md^2 N) / (V + N).  Identical
-        // inputs give V = md = 0 and an SSIM of exactly 0.
-        const float md = m1 - m2;
-        const float md2 = md * md;
-        const float N = fmaf(2.0f, s12 - m1 * m2, 0.0009f);
-        const float V = D - md2;
-        const float ssim = fmaxf(fmaf(md2, N, V) / (V + N), 0.0f);
-        // Artifact and detail-loss maps (score.hpp:276-281): (|b-mu2|+1)/(|a-mu1|+1) - 1,
-        // evaluated as (|b-mu2| - |a-mu1|) / (|a-mu1| + 1) to avoid cancelling against 1.
-        const float ca = sa[r0 + o + kHalo][c + kHalo], cb = sb[r0 + o + kHalo][c + kHalo];
-        const float ea = fabsf(ca - m1), eb = fabsf(cb - m2);
-        const float v1 = (eb - ea) / (ea + 1.0f);
-        const float art = fmaxf(v1, 0.0f), det = fmaxf(-v1, 0.0f);
-        const float s2 = ssim * ssim, a2 = art * art, d2 = det * det;
-        sum[0] += ssim; sum[1] += art; sum[2] += det;
-        sum[3] += s2 * s2; sum[4] += a2 * a2; sum[5] += d2 * d2;
-    }
-    // FP64 tree reduction of the tile.
-    double dsum[6];
+        for (int q = 0; q < 6; q++) {
+            double v = (double)sum[q];
 #pragma unroll
-    for (int q = 0; q < 6; q++) {
-        double v = (double)sum[q];
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            dsum[q] = v;
+        }
+        const int warp = tid >> 5, lane = tid & 31;
+        if (lane == 0) {
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        dsum[q] = v;
-    }
-    const int warp = tid >> 5, lane = tid & 31;
-    if (lane == 0) {
+            for (int q = 0; q < 6; q++) red[warp][q] = dsum[q];
+        }
+        __syncthreads();
+        if (tid < 6) {
+            double v = 0.0;
 #pragma unroll
-        for (int q = 0; q < 6; q++) red[warp][q] = dsum[q];
-    }
-    __syncthreads();
-    if (tid < 6) {
-        double v = 0.0;
-#pragma unroll
-        for (int w = 0; w < kMapThreads / 32; w++) v += red[w][tid];
-        partials[(int64_t)blockIdx.x * 6 + tid] = v;
+            for (int wi = 0; wi < kMapThreads / 32; wi++) v += red[wi][tid];
+            partials[(int64_t)tile * 6 + tid] = v;
+        }
+        if (next >= total_tiles) break;
+        tile = next;
+        __syncthreads();
     }
 }
 
@@ -469,6 +540,45 @@ static void upload_gauss_constants() {
     CUDA_CHECK(cudaMemcpyToSymbol(c_gauss_prefix, pre, sizeof(pre)));
 }
 
+// Launches the front kernel on raw inputs, specialised when both clips share a fast format.
+static void launch_front(const FrontArgs& fa, const ColourParams cp[2], dim3 grid, cudaStream_t st, KernelTimer* timer) {
+    const int smem = (int)sizeof(float) * std::max(chroma_stage_floats(cp[0].subw, cp[0].subh),
+                                                   chroma_stage_floats(cp[1].subw, cp[1].subh));
+    const int f0 = fast_path_of(cp[0]), f1 = fast_path_of(cp[1]);
+    const int fast = f0 == f1 ? f0 : kFastGeneric;
+    auto kern = fast == kFastYuv420Bt709 ? ssimu2_front_kernel<false, kFastYuv420Bt709>
+              : fast == kFastRgb8Srgb ? ssimu2_front_kernel<false, kFastRgb8Srgb>
+                                      : ssimu2_front_kernel<false, kFastGeneric>;
+    if (smem > 32 * 1024) CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int t = timer ? timer->begin(0, "ssimu2_front", st) : -1;
+    kern<<<grid, 256, smem, st>>>(fa);
+    CUDA_CHECK(cudaGetLastError());
+    if (timer) timer->end(t, st);
+}
+
+// Work-list template of one pair for the maps kernel (same order as the per-pair segments
+// of build_segments, which the final kernel walks).
+static MapTemplate make_map_template(const Pyramid& pyr, const float* xyb) {
+    MapTemplate mt{};
+    int tile = 0;
+    for (int s = 0; s < kScales; s++)
+        for (int p = 0; p < 3; p++) {
+            if (!plane_needed(p, s)) continue;
+            MapTemplate::Seg& g = mt.seg[mt.nseg++];
+            g.off = pyr.off[s][p];
+            g.w = pyr.w[s];
+            g.h = pyr.h[s];
+            g.pitch = pyr.pitch[s];
+            g.tiles_x = (int)ceil_div(g.w, kTile);
+            g.tile_begin = tile;
+            tile += g.tiles_x * (int)ceil_div(g.h, kTile);
+        }
+    mt.tiles_per_pair = tile;
+    mt.xyb = xyb;
+    mt.image_floats = pyr.image_floats;
+    return mt;
+}
+
 class Engine final : public Ssimu2Api {
 public:
     ~Engine() override { release(); }
@@ -490,25 +600,27 @@ public:
         CUDA_CHECK(cudaEventCreateWithFlags(&last_done_, cudaEventDisableTiming));
         upload_gauss_constants();
         for (int c = 0; c < 2; c++) {
-            staged_bytes_[c] = dense_image_bytes(geo_[c], staged_off_[c]);
-            staged_[c] = device_alloc<uint8_t>((size_t)staged_bytes_[c], "input staging");
+            int64_t off[3];
+            staging_[c].ensure((size_t)dense_image_bytes(geo_[c], off), stream_);
             if (generic_) lin_[c].alloc(geo_[c]);
         }
         score_host_ = pinned_alloc<double>(1, "score");
+        int sms = 0, per_sm = 0;
+        CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ssimu2_maps_kernel, kMapThreads, 0));
+        maps_grid_ = std::max(1, sms * std::max(1, per_sm));
         ensure_capacity(1);
     }
 
     double compute(const uint8_t* const s1[3], const uint8_t* const s2[3], const int64_t ls1[3], const int64_t ls2[3]) override {
         CUDA_CHECK(cudaStreamWaitEvent(stream_, last_done_, 0));
-        stage_host_image(staged_[0], staged_off_[0], geo_[0], s1, ls1, stream_);
-        stage_host_image(staged_[1], staged_off_[1], geo_[1], s2, ls2, stream_);
         RawImage raw[2];
-        for (int c = 0; c < 2; c++)
-            for (int p = 0; p < 3; p++) {
-                raw[c].p[p] = staged_[c] + staged_off_[c][p];
-                raw[c].stride[p] = geo_[c].pw[p] * geo_[c].bytes;
-            }
-        run_pairs(1, raw, cp_, stream_, scores_d_, features_d_);
+        ColourParams cp[2] = {cp_[0], cp_[1]};
+        for (int c = 0; c < 2; c++) {
+            raw[c] = stage_host_image(staging_[c], geo_[c], c ? s2 : s1, c ? ls2 : ls1, stream_);
+            cp[c].misaligned = misaligned_view(raw[c], geo_[c]) ? 1 : 0;
+        }
+        run_pairs(1, raw, cp, stream_, scores_d_, features_d_);
         CUDA_CHECK(cudaMemcpyAsync(score_host_, scores_d_, sizeof(double), cudaMemcpyDeviceToHost, stream_));
         CUDA_CHECK(cudaMemcpyAsync(last_features_, features_d_, sizeof(float) * 108, cudaMemcpyDeviceToHost, stream_));
         CUDA_CHECK(cudaEventRecord(last_done_, stream_));
@@ -643,6 +755,7 @@ private:
         features_d_ = device_alloc<float>((size_t)108 * ncap, "features");
         const std::vector<MapSeg> segs = build_segments(ncap);
         CUDA_CHECK(cudaMemcpy(segs_d_, segs.data(), segs.size() * sizeof(MapSeg), cudaMemcpyHostToDevice));
+        map_template_ = make_map_template(pyr_, xyb_);
         cap_ = ncap;
     }
 
@@ -657,14 +770,7 @@ private:
         for (int i = 0; i < nimg; i++) fa->raw[i] = raw[i];
         const dim3 fgrid((unsigned)ceil_div(pyr_.w[1], 32), (unsigned)ceil_div(pyr_.h[1], 32), (unsigned)nimg);
         if (!generic_) {
-            const int smem = (int)sizeof(float) * std::max(chroma_stage_floats(cp[0].subw, cp[0].subh),
-                                                           chroma_stage_floats(cp[1].subw, cp[1].subh));
-            if (smem > 32 * 1024)
-                CUDA_CHECK(cudaFuncSetAttribute(ssimu2_front_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            const int t = timer_.begin(0, "ssimu2_front", st);
-            ssimu2_front_kernel<false><<<fgrid, 256, smem, st>>>(*fa);
-            CUDA_CHECK(cudaGetLastError());
-            timer_.end(t, st);
+            launch_front(*fa, cp, fgrid, st, &timer_);
         } else {
             // Resize/crop path (one pair): planar linear RGB first, then the pyramid reads the
             // crop window of each clip.
@@ -674,12 +780,12 @@ private:
                 fa->lin_plane[c] = geo_[c].TW * geo_[c].TH;
                 fa->lin_pitch[c] = geo_[c].TW;
             }
-            ssimu2_front_kernel<true><<<fgrid, 256, 0, st>>>(*fa);
+            ssimu2_front_kernel<true, kFastGeneric><<<fgrid, 256, 0, st>>>(*fa);
             CUDA_CHECK(cudaGetLastError());
         }
         const int ntiles = tiles_per_pair_ * npairs;
         const int t1 = timer_.begin(1, "ssimu2_maps", st);
-        ssimu2_maps_kernel<<<(unsigned)ntiles, kMapThreads, 0, st>>>(segs_d_, segs_per_pair_ * npairs, partials_);
+        ssimu2_maps_kernel<<<(unsigned)std::min(ntiles, maps_grid_), kMapThreads, 0, st>>>(map_template_, ntiles, partials_);
         CUDA_CHECK(cudaGetLastError());
         timer_.end(t1, st);
         const int t2 = timer_.begin(2, "ssimu2_final", st);
@@ -692,8 +798,7 @@ private:
         if (stream_) (void)cudaStreamSynchronize(stream_);
         timer_.destroy();
         for (int c = 0; c < 2; c++) {
-            device_free(staged_[c]);
-            staged_[c] = nullptr;
+            staging_[c].free();
             lin_[c].free();
         }
         device_free(xyb_);
@@ -723,9 +828,7 @@ private:
     int tiles_per_pair_ = 0, segs_per_pair_ = 0;
     int width_ = 0, height_ = 0;
     cudaStream_t stream_ = nullptr;
-    uint8_t* staged_[2] = {nullptr, nullptr};
-    int64_t staged_off_[2][3] = {};
-    int64_t staged_bytes_[2] = {0, 0};
+    StagingBuffer staging_[2];
     GenericLinear lin_[2];
     float* xyb_ = nullptr;
     double* partials_ = nullptr;
@@ -736,6 +839,8 @@ private:
     float last_features_[108] = {};
     int cap_ = 0;
     FrontArgs front_args_{};
+    MapTemplate map_template_{};
+    int maps_grid_ = 0;
     cudaEvent_t last_done_ = nullptr;  // completion of the previous call, on whichever stream it ran
     KernelTimer timer_;
 };
@@ -887,14 +992,14 @@ static void compute_no_alloc(const Vship_Colorspace_t& src, const Vship_Colorspa
             fa.raw[c].p[p] = (c ? d2 : d1)[p];
             fa.raw[c].stride[p] = (c ? ls2 : ls1)[p];
         }
-    const int smem = (int)sizeof(float) * std::max(chroma_stage_floats(cp[0].subw, cp[0].subh),
-                                                   chroma_stage_floats(cp[1].subw, cp[1].subh));
-    if (smem > 32 * 1024)
-        CUDA_CHECK(cudaFuncSetAttribute(ssimu2_front_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const dim3 fgrid((unsigned)ceil_div(pyr.w[1], 32), (unsigned)ceil_div(pyr.h[1], 32), 2u);
-    ssimu2_front_kernel<false><<<fgrid, 256, smem, st>>>(fa);
-    CUDA_CHECK(cudaGetLastError());
-    ssimu2_maps_kernel<<<(unsigned)ntiles, kMapThreads, 0, st>>>(segs_d, nsegs, partials);
+    launch_front(fa, cp, fgrid, st, nullptr);
+    const MapTemplate mt = make_map_template(pyr, xyb);
+    int sms = 0, per_sm = 0, dev = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ssimu2_maps_kernel, kMapThreads, 0));
+    ssimu2_maps_kernel<<<(unsigned)std::min(ntiles, std::max(1, sms * per_sm)), kMapThreads, 0, st>>>(mt, ntiles, partials);
     CUDA_CHECK(cudaGetLastError());
     ssimu2_final_kernel<<<1, 256, 0, st>>>(segs_d, nsegs, partials, d_score, d_features);
     CUDA_CHECK(cudaGetLastError());
