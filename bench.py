@@ -378,6 +378,81 @@ def run_reference(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+BW, BH, BBATCH = 3840, 2160, 32
+BWORKLOAD = "butteraugli_4k_srgb8_batch32_q5_i203_distmap"
+BMETRIC = "4K Butteraugli frame-pairs/s"
+# Algorithmic bytes per 4K Butteraugli pair (FP32 staged model, see DESIGN.md "Roofline").
+B_ALGO_BYTES = 2_903_040_000
+
+
+def run_butteraugli(args, world, rank, local):
+    """Secondary line: Butteraugli on 4K 8-bit sRGB pairs (intensity 203, Q-norm 5, distortion
+    map returned), device-resident and end to end through Vship_ComputeButteraugli."""
+    import torch
+    from vship_b200 import abi, api, synth
+    torch.cuda.set_device(local)
+    t = time.time()
+    pairs = synth.make_pairs(BBATCH, BW, BH, fmt="rgb8", seed=77 + rank, unique=4, blur=(0.0, 1.5))
+    log("generated %d 4K pairs in %.1fs" % (len(pairs), time.time() - t))
+    cs = abi.srgb8(BW, BH)
+    ls = pairs[0][2]
+    dev = [([torch.from_numpy(p).cuda() for p in a], [torch.from_numpy(p).cuda() for p in b]) for a, b, _ in pairs]
+    norms = torch.zeros(BBATCH, 3, dtype=torch.float64, device="cuda")
+    dmap = torch.zeros(BH, BW, dtype=torch.float32, device="cuda")
+    h = api.Butteraugli(cs, qnorm=5, intensity=203.0, gpu_id=local)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        for i, (d1, d2) in enumerate(dev):
+            h.compute_device([x.data_ptr() for x in d1], [x.data_ptr() for x in d2], ls, ls,
+                             norms[i].data_ptr(), dmap.data_ptr(), BW * 4, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    value = BBATCH * args.steps / (ms / 1e3)
+    h.kernel_timing(True)
+    h.kernel_times(reset=True)
+    step()
+    torch.cuda.synchronize()
+    ktimes = h.kernel_times(reset=True)
+    h.kernel_timing(False)
+    per_pair_ms = {k: round(v[1] / BBATCH, 4) for k, v in ktimes.items()}
+    pinned, host_pairs = pinned_frames(pairs, api)
+    out = np.zeros((BH, BW), np.float32)
+    h.compute(host_pairs[0][0], host_pairs[0][1], ls, ls)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for i in range(BBATCH):
+            res, _ = h.compute(host_pairs[i][0], host_pairs[i][1], ls, ls, distmap=True)
+    e2e_s = time.perf_counter() - t0
+    h.close()
+    for pb in pinned:
+        pb.free()
+    peak, peak_kind = measured_peaks()
+    achieved = B_ALGO_BYTES / (sum(v[1] for v in ktimes.values()) / BBATCH / 1e3) / 1e9
+    line = {"metric": BMETRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": BWORKLOAD, "pairs_per_step": BBATCH, "width": BW, "height": BH},
+            "e2e": {"value": round(BBATCH * args.steps / e2e_s, 2), "unit": UNIT,
+                    "api": "Vship_ComputeButteraugli with distortion map, one thread",
+                    "h2d_bytes_per_step": BBATCH * 2 * 3 * BW * BH, "d2h_bytes_per_step": BBATCH * (BW * BH * 4 + 24)},
+            "kernels_ms_per_pair": per_pair_ms,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": peak_kind,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_pair": B_ALGO_BYTES, "scope": "whole pipeline"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_profile_case(args):
     """Small device-resident run for ncu captures: `--profile-pairs` 1080p pairs, `--steps`
     calls of VshipExt_ComputeSSIMU2Device, nothing else (no timing, no e2e, no CPU leg)."""
@@ -410,6 +485,8 @@ def main():
     ap.add_argument("--ref-threads", type=int, nargs="+", default=[1, 3, 4, 8])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli"],
+                    help="butteraugli: secondary 4K Butteraugli line instead of the headline metric")
     ap.add_argument("--profile-pairs", type=int, default=0,
                     help="only run N device-resident pairs --steps times (for ncu captures)")
     args = ap.parse_args()
@@ -419,6 +496,10 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_env()
+    if args.metric == "butteraugli":
+        if args.impl == "ours" and rank == 0:
+            run_butteraugli(args, world, rank, local)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank, local)
     else:
