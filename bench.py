@@ -453,6 +453,284 @@ def run_butteraugli(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+UNEVEN_RES = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
+UNEVEN_N = 256
+UWORKLOAD = "ssimu2_uneven_256_srgb8_360p_720p_1080p_4k"
+UMETRIC = "uneven-resolution SSIMU2 frame-pairs/s"
+
+
+def xyb_floats(w, h):
+    """Floats of the XYB planes some map reads, for a w x h image (Y at level 0; X, Y at
+    levels 1-2; X, Y, B at levels 3-4)."""
+    sizes = [(w, h)]
+    for _ in range(5):
+        pw, ph = sizes[-1]
+        sizes.append(((pw - 1) // 2 + 1, (ph - 1) // 2 + 1))
+    planes = [1, 2, 2, 3, 3, 0]
+    return sum(n * sw * sh for n, (sw, sh) in zip(planes, sizes))
+
+
+def make_uneven(seed):
+    """256 pairs with resolutions drawn uniformly from UNEVEN_RES (seeded), 8-bit sRGB, content
+    and DCT distortion as the headline workload; 8 distinct pairs per resolution are cycled."""
+    from vship_b200 import synth
+    rng = np.random.default_rng(seed)
+    draw = rng.integers(0, len(UNEVEN_RES), UNEVEN_N)
+    t = time.time()
+    gen = {}
+    for k, (w, h) in enumerate(UNEVEN_RES):
+        gen[k] = synth.make_pairs(8, w, h, fmt="rgb8", seed=seed + 17 * k, unique=4, steps=(4.0, 48.0))
+    pairs = []
+    seen = {k: 0 for k in gen}
+    for k in draw:
+        p1, p2, ls = gen[int(k)][seen[int(k)] % 8]
+        seen[int(k)] += 1
+        pairs.append((UNEVEN_RES[int(k)], p1, p2, ls))
+    log("generated %d uneven pairs in %.1fs (%s)" % (len(pairs), time.time() - t,
+                                                     {"%dx%d" % UNEVEN_RES[k]: seen[k] for k in seen}))
+    return pairs
+
+
+def uneven_pinned(pairs, api, lib=None):
+    """Each frame of the uneven workload in one pinned buffer (FFVship layout)."""
+    pinned, host = [], []
+    for (wh, p1, p2, ls) in pairs:
+        frames = []
+        for planes in (p1, p2):
+            nbytes = sum(p.nbytes for p in planes)
+            pb = api.PinnedBuffer(nbytes, lib=lib)
+            off, ptrs = 0, []
+            for p in planes:
+                pb.array[off:off + p.nbytes] = p.reshape(-1)
+                ptrs.append(pb.ptr.value + off)
+                off += p.nbytes
+            pinned.append(pb)
+            frames.append(ptrs)
+        host.append((wh, frames[0], frames[1], ls))
+    return pinned, host
+
+
+def run_uneven(args, world, rank, local):
+    """Uneven batch: 256 pairs of mixed resolutions scored in one persistent launch replayed
+    from a CUDA graph (VshipExt_ComputeSSIMU2BatchDevice), against per-frame launches and
+    per-resolution batched launches of the per-handler path."""
+    import torch
+    from vship_b200 import abi, api
+    torch.cuda.set_device(local)
+    pairs = make_uneven(seed=4321 + rank)
+    n = len(pairs)
+    cs = {wh: abi.srgb8(*wh) for wh in UNEVEN_RES}
+    dev = [(wh, [torch.from_numpy(p).cuda() for p in p1], [torch.from_numpy(p).cuda() for p in p2], ls)
+           for wh, p1, p2, ls in pairs]
+    items = [(cs[wh], cs[wh], [t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls, ls) for wh, d1, d2, ls in dev]
+    arr, keep = api.frame_pairs(items)
+    scores = torch.zeros(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    b = api.SSIMU2Batch(gpu_id=local)
+    if args.tile_rows:
+        b.set_tile_rows(args.tile_rows)
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def batch_step():
+        b.compute_device_array(arr, n, scores.data_ptr(), 0, stream.cuda_stream)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ms = timed(batch_step, args.steps)
+    clocks = sampler.stop()
+    value = n * args.steps / (ms / 1e3)
+    rows = b.tile_rows()
+    batch_scores = scores.cpu().numpy().copy()
+    # tile-height sweep (the autotuner's candidates), timed the same way
+    sweep = {}
+    for r in (16, 32, 64):
+        b.set_tile_rows(r)
+        sweep[r] = round(n * 3 / (timed(batch_step, 3) / 1e3), 1)
+    b.set_tile_rows(args.tile_rows or 0)
+    b.kernel_timing(True)
+    b.kernel_times(reset=True)
+    for _ in range(3):
+        batch_step()
+    torch.cuda.synchronize()
+    kt = b.kernel_times(reset=True)
+    b.kernel_timing(False)
+    launches, total_ms = kt["ssimu2_batch"]
+    avg_ms = total_ms / launches
+    algo = sum(2 * (3 * w * h + 8 * xyb_floats(w, h)) for (w, h), _, _, _ in pairs)
+    peak, peak_kind = measured_peaks()
+    achieved = algo / (avg_ms / 1e3) / 1e9
+
+    # per-frame launches: one handler per resolution, one pair per call
+    handlers = {wh: api.SSIMU2(cs[wh], gpu_id=local) for wh in UNEVEN_RES}
+    pf_scores = torch.zeros(n, dtype=torch.float64, device="cuda")
+    pf_args = [(handlers[wh], [t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls) for wh, d1, d2, ls in dev]
+
+    def per_frame_step():
+        for i, (hh, a1, a2, ls) in enumerate(pf_args):
+            hh.compute_device(1, a1, a2, ls, ls, pf_scores[i].data_ptr(), 0, stream.cuda_stream)
+
+    pf_ms = timed(per_frame_step, max(1, args.steps // 2))
+    per_frame = n * max(1, args.steps // 2) / (pf_ms / 1e3)
+    max_diff = float(np.max(np.abs(pf_scores.cpu().numpy() - batch_scores)))
+
+    # per-resolution batches: each handler scores all pairs of its resolution per call
+    groups = {}
+    for i, (wh, d1, d2, ls) in enumerate(dev):
+        groups.setdefault(wh, []).append(i)
+    grp_args = []
+    for wh, idx in groups.items():
+        a1 = [t.data_ptr() for i in idx for t in dev[i][1]]
+        a2 = [t.data_ptr() for i in idx for t in dev[i][2]]
+        out = torch.zeros(len(idx), dtype=torch.float64, device="cuda")
+        grp_args.append((handlers[wh], len(idx), a1, a2, dev[idx[0]][3], out))
+
+    def per_class_step():
+        for hh, k, a1, a2, ls, out in grp_args:
+            hh.compute_device(k, a1, a2, ls, ls, out.data_ptr(), 0, stream.cuda_stream)
+
+    pc_ms = timed(per_class_step, max(1, args.steps // 2))
+    per_class = n * max(1, args.steps // 2) / (pc_ms / 1e3)
+    for hh in handlers.values():
+        hh.close()
+
+    # end to end: host API of the batch handler with each frame in one pinned buffer
+    pinned, host = uneven_pinned(pairs, api)
+    host_items = [(cs[wh], cs[wh], f1, f2, ls, ls) for wh, f1, f2, ls in host]
+    harr, hkeep = api.frame_pairs(host_items)
+    e2e_scores = np.zeros(n)
+    import ctypes as _ct
+    L = api.load()
+
+    def e2e_step():
+        rc = L.VshipExt_ComputeSSIMU2Batch(b.h, n, harr, e2e_scores.ctypes.data_as(_ct.POINTER(_ct.c_double)), None)
+        if rc != 0:
+            raise RuntimeError("VshipExt_ComputeSSIMU2Batch failed: %d" % rc)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, args.steps // 2)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    e2e_diff = float(np.max(np.abs(e2e_scores - batch_scores)))
+    in_bytes = sum(p.nbytes for _, p1, p2, _ in pairs for p in p1 + p2)
+    for pb in pinned:
+        pb.free()
+    b.close()
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+        oracle.build()
+        k, t0, maxd = 0, time.perf_counter(), 0.0
+        while k < n and time.perf_counter() - t0 < args.cpu_seconds:
+            wh, p1, p2, ls = pairs[k]
+            q, d, _ = oracle.ssimu2(oracle.convert(p1, ls, cs[wh]), oracle.convert(p2, ls, cs[wh]))
+            maxd = max(maxd, abs(batch_scores[k] - d))
+            k += 1
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(k / dt, 3), "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+               "sample": "first %d pairs of the uneven workload in FP64 (%.1f s)" % (k, dt),
+               "max_abs_dscore_gpu_vs_fp64": maxd}
+    line = {
+        "metric": UMETRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": UWORKLOAD, "pairs_per_step": n, "resolutions": ["%dx%d" % r for r in UNEVEN_RES],
+                   "format": "8-bit sRGB", "tile_rows": rows, "launch": "one persistent launch per step (CUDA graph)",
+                   "l2": "inputs (%.0f MB per step) larger than L2" % (in_bytes / 1e6)},
+        "per_frame_value": round(per_frame, 2), "per_class_value": round(per_class, 2),
+        "tile_rows_sweep": sweep, "max_abs_score_diff_vs_per_frame": max_diff,
+        "e2e": {"value": round(n * e2e_steps / e2e_s, 2), "unit": UNIT,
+                "api": "VshipExt_ComputeSSIMU2Batch, each frame in one pinned buffer",
+                "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": n * 8,
+                "max_abs_score_diff_vs_device_path": e2e_diff},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "kernel": "ssimu2_batch", "achieved": round(achieved, 1), "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(avg_ms, 4)},
+        "cpu_baseline": cpu, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_uneven_reference(args, world, rank, local):
+    """Reference arm of the uneven workload: the reference library, one handler per resolution
+    per host thread, one pair per call through Vship_ComputeSSIMU2 with pinned frames."""
+    if rank != 0:
+        return
+    from vship_b200 import abi, api
+    ref = os.path.join(ROOT, "oracle", "_ref", "libvship_ref.so")
+    if not os.path.exists(ref):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libvship_ref.so was not built"}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    L = api.load_library(ref)
+    pairs = make_uneven(seed=4321)
+    n = len(pairs)
+    cs = {wh: abi.srgb8(*wh) for wh in UNEVEN_RES}
+    pinned, host = uneven_pinned(pairs, api, lib=L)
+    best = None
+    for nthreads in args.ref_threads:
+        handlers = [{wh: api.SSIMU2(cs[wh], gpu_id=local, lib=L) for wh in UNEVEN_RES} for _ in range(nthreads)]
+        out = np.zeros(n)
+
+        def worker(k):
+            torch.cuda.set_device(local)
+            for i in range(k, n, nthreads):
+                wh, f1, f2, ls = host[i]
+                out[i] = handlers[k][wh].compute(f1, f2, ls, ls)
+
+        def step():
+            ths = [threading.Thread(target=worker, args=(k,)) for k in range(nthreads)]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+
+        for _ in range(args.warmup):
+            step()
+        t0 = time.perf_counter()
+        steps = max(1, args.steps // 2)
+        for _ in range(steps):
+            step()
+        dt = time.perf_counter() - t0
+        v = n * steps / dt
+        log("reference uneven: %d threads -> %.1f pairs/s" % (nthreads, v))
+        if best is None or v > best[0]:
+            best = (v, nthreads, dt / steps)
+        for hs in handlers:
+            for hh in hs.values():
+                hh.close()
+    for pb in pinned:
+        pb.free()
+    v, nthreads, dt = best
+    print(json.dumps({
+        "impl": "reference", "metric": UMETRIC, "value": round(v, 2), "unit": UNIT, "n_gpus": 1,
+        "steps": max(1, args.steps // 2), "warmup": args.warmup, "ms_per_step": round(dt * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": UWORKLOAD, "pairs_per_step": n, "threads_handlers": nthreads,
+                   "api": "Vship_ComputeSSIMU2 per pair, one handler per resolution per thread"},
+        "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "kind": "reference", "cores": nthreads,
+                         "sample": "the reference's CUDA build on the B200 driven by %d host threads" % nthreads}}),
+        flush=True)
+
+
 def run_profile_case(args):
     """Small device-resident run for ncu captures: `--profile-pairs` 1080p pairs, `--steps`
     calls of VshipExt_ComputeSSIMU2Device, nothing else (no timing, no e2e, no CPU leg)."""
@@ -475,6 +753,44 @@ def run_profile_case(args):
     log("profile case: %d pairs x %d calls, scores %s" % (n, args.steps, np.round(scores.cpu().numpy()[:4], 4)))
 
 
+def run_profile_uneven(args):
+    """Small uneven case for ncu captures: `--profile-uneven` pairs drawn like the uneven
+    workload, scored `--steps` times by the batch graph (32-row tiles), then once per
+    resolution by the per-handler path.  No timing."""
+    import torch
+    from vship_b200 import abi, api, synth
+    rng = np.random.default_rng(4321)
+    draw = rng.integers(0, len(UNEVEN_RES), args.profile_uneven)
+    gen = {k: synth.make_pairs(2, w, h, fmt="rgb8", seed=5 + k, unique=1) for k, (w, h) in enumerate(UNEVEN_RES)}
+    dev = []
+    for i, k in enumerate(draw):
+        p1, p2, ls = gen[int(k)][i % 2]
+        dev.append((UNEVEN_RES[int(k)], [torch.from_numpy(p).cuda() for p in p1], [torch.from_numpy(p).cuda() for p in p2], ls))
+    cs = {wh: abi.srgb8(*wh) for wh in UNEVEN_RES}
+    items = [(cs[wh], cs[wh], [t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls, ls) for wh, d1, d2, ls in dev]
+    n = len(items)
+    scores = torch.zeros(n, dtype=torch.float64, device="cuda")
+    with api.SSIMU2Batch() as b:
+        b.set_tile_rows(32)
+        for _ in range(args.steps):
+            b.compute_device(items, scores.data_ptr())
+        torch.cuda.synchronize()
+    batch = scores.cpu().numpy().copy()
+    groups = {}
+    for i, (wh, d1, d2, ls) in enumerate(dev):
+        groups.setdefault(wh, []).append(i)
+    for wh, idx in groups.items():
+        with api.SSIMU2(cs[wh]) as h:
+            out = torch.zeros(len(idx), dtype=torch.float64, device="cuda")
+            h.compute_device(len(idx), [t.data_ptr() for i in idx for t in dev[i][1]],
+                             [t.data_ptr() for i in idx for t in dev[i][2]], dev[idx[0]][3], dev[idx[0]][3],
+                             out.data_ptr(), 0, 0)
+            torch.cuda.synchronize()
+            scores[idx] = out
+    log("profile uneven: %d pairs, max |batch - per-class| = %.3g" %
+        (n, float(np.max(np.abs(scores.cpu().numpy() - batch)))))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,13 +801,21 @@ def main():
     ap.add_argument("--ref-threads", type=int, nargs="+", default=[1, 3, 4, 8])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli"],
-                    help="butteraugli: secondary 4K Butteraugli line instead of the headline metric")
+    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli", "ssimu2-uneven"],
+                    help="butteraugli: secondary 4K Butteraugli line; ssimu2-uneven: 256 pairs of mixed "
+                         "resolutions in one persistent launch, instead of the headline metric")
+    ap.add_argument("--tile-rows", type=int, default=0, help="ssimu2-uneven: fixed map tile rows (0: autotune)")
     ap.add_argument("--profile-pairs", type=int, default=0,
                     help="only run N device-resident pairs --steps times (for ncu captures)")
+    ap.add_argument("--profile-uneven", type=int, default=0,
+                    help="only run N uneven pairs through the batch graph --steps times and once per "
+                         "resolution through handlers (for ncu captures)")
     args = ap.parse_args()
     if args.profile_pairs:
         run_profile_case(args)
+        return
+    if args.profile_uneven:
+        run_profile_uneven(args)
         return
     if args.warmup < 3:
         args.warmup = 3
@@ -499,6 +823,12 @@ def main():
     if args.metric == "butteraugli":
         if args.impl == "ours" and rank == 0:
             run_butteraugli(args, world, rank, local)
+        return
+    if args.metric == "ssimu2-uneven":
+        if args.impl == "reference":
+            run_uneven_reference(args, world, rank, local)
+        elif rank == 0:
+            run_uneven(args, world, rank, local)
         return
     if args.impl == "reference":
         run_reference(args, world, rank, local)

@@ -81,6 +81,63 @@ EXPORTPREPROCESS Vship_Exception VshipExt_ComputeSSIMU2NoAlloc(Vship_Colorspace_
                                                                 const uint8_t* const srcp2[3], const int64_t lineSize[3],
                                                                 const int64_t lineSize2[3], void* stream);
 
+/* ---- Uneven batches --------------------------------------------------------------------
+ * No counterpart in the reference, which scores one pair per call through a handler bound to
+ * one colourspace pair.  A batch handler scores any number of pairs whose colourspaces may
+ * all differ (resolutions, formats) in one persistent launch replayed from a CUDA graph: one
+ * work list holds the front tiles of every image, then the map tiles of every pair, then
+ * each pair's final reduction, and a map tile starts once both pyramids of its pair are
+ * built.  Resize and crop (target_width/height other than -1, or a non-zero crop) are not
+ * supported in batches; use a per-colourspace handler for those. */
+
+/* One frame pair of a batch: both colourspaces, three plane pointers per image and the row
+ * strides in bytes (device pointers for VshipExt_ComputeSSIMU2BatchDevice, host pointers for
+ * VshipExt_ComputeSSIMU2Batch). */
+typedef struct VshipExt_FramePair {
+    Vship_Colorspace_t src_colorspace;
+    Vship_Colorspace_t dis_colorspace;
+    const uint8_t* srcp1[3];
+    const uint8_t* srcp2[3];
+    int64_t lineSize[3];
+    int64_t lineSize2[3];
+} VshipExt_FramePair;
+
+typedef struct VshipExt_SSIMU2BatchHandler {
+    unsigned int id;
+} VshipExt_SSIMU2BatchHandler;
+
+EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchInit(VshipExt_SSIMU2BatchHandler* handler, int gpu_id);
+EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchFree(VshipExt_SSIMU2BatchHandler handler);
+EXPORTPREPROCESS int VshipExt_SSIMU2BatchGetDetailedLastError(VshipExt_SSIMU2BatchHandler handler, char* out_message, int len);
+
+/* n device-resident pairs, queued on `stream` (NULL: the legacy default stream) without
+ * waiting.  d_scores (device, n doubles) receives the scores, d_features (device, 108 n
+ * floats, may be NULL) the features.  Device buffers grow to the largest batch seen
+ * (allocation synchronises the device).  With automatic tile rows (the default) the first
+ * batch of a new mix of resolutions times each tile shape and synchronises; do that before
+ * any stream capture, or fix the rows with VshipExt_SSIMU2BatchSetTileRows.  Wait-time
+ * limits inside the launch are reported by the next call on the handler. */
+EXPORTPREPROCESS Vship_Exception VshipExt_ComputeSSIMU2BatchDevice(VshipExt_SSIMU2BatchHandler handler, int n,
+                                                                    const VshipExt_FramePair* pairs, double* d_scores,
+                                                                    float* d_features, void* stream);
+/* n host-resident pairs (pageable or pinned): copies them in chunks that overlap with the
+ * scoring of the previous chunk, writes n scores (host) and, when features is not NULL,
+ * 108 n features (host), and returns when they are written. */
+EXPORTPREPROCESS Vship_Exception VshipExt_ComputeSSIMU2Batch(VshipExt_SSIMU2BatchHandler handler, int n,
+                                                              const VshipExt_FramePair* pairs, double* scores,
+                                                              float* features);
+/* Rows of the map tiles: 16, 32 or 64, or 0 to choose by timing (the default).  Timed
+ * choices are kept per device and mix of resolutions in memory and in the JSON file named by
+ * the VSHIP_TUNE_CACHE environment variable (default
+ * $XDG_CACHE_HOME/vship_b200/ssimu2_tiles.json or ~/.cache/vship_b200/ssimu2_tiles.json;
+ * an empty value disables the file). */
+EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchSetTileRows(VshipExt_SSIMU2BatchHandler handler, int rows);
+/* Rows used by the last batch (0 before the first). */
+EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchTileRows(VshipExt_SSIMU2BatchHandler handler, int* rows);
+EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchKernelTiming(VshipExt_SSIMU2BatchHandler handler, int enable);
+EXPORTPREPROCESS int VshipExt_SSIMU2BatchKernelTimes(VshipExt_SSIMU2BatchHandler handler, VshipExt_KernelTime* out,
+                                                     int max, int reset);
+
 /* Metric resolution (after resize and crop) of a handler. */
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2Resolution(Vship_SSIMU2Handler handler, int64_t* width, int64_t* height);
 EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliResolution(Vship_ButteraugliHandler handler, int64_t* width, int64_t* height);

@@ -121,9 +121,11 @@ def test_struct_layouts_match_c():
 #include <stdio.h>
 #include <stddef.h>
 #include "VshipAPI.h"
+#include "VshipAPI_ext.h"
 int main(void){
- printf("%zu %zu %zu %zu %zu %zu\n", sizeof(Vship_Colorspace_t), offsetof(Vship_Colorspace_t, sample),
-        offsetof(Vship_Colorspace_t, crop), sizeof(Vship_DeviceInfo), sizeof(Vship_ButteraugliScore), sizeof(Vship_Version));
+ printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(Vship_Colorspace_t), offsetof(Vship_Colorspace_t, sample),
+        offsetof(Vship_Colorspace_t, crop), sizeof(Vship_DeviceInfo), sizeof(Vship_ButteraugliScore), sizeof(Vship_Version),
+        sizeof(VshipExt_FramePair), offsetof(VshipExt_FramePair, srcp1), offsetof(VshipExt_FramePair, lineSize2));
  return 0;}
 '''
     import tempfile
@@ -134,4 +136,5 @@ int main(void){
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         vals = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
     assert vals == [ctypes.sizeof(abi.Colorspace), abi.Colorspace.sample.offset, abi.Colorspace.crop.offset,
-                    ctypes.sizeof(abi.DeviceInfo), ctypes.sizeof(abi.ButteraugliScore), ctypes.sizeof(abi.Version)]
+                    ctypes.sizeof(abi.DeviceInfo), ctypes.sizeof(abi.ButteraugliScore), ctypes.sizeof(abi.Version),
+                    ctypes.sizeof(abi.FramePair), abi.FramePair.srcp1.offset, abi.FramePair.lineSize2.offset]

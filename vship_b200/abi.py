@@ -131,3 +131,15 @@ class ButteraugliScore(ctypes.Structure):
 
 PlanePtrs = ctypes.POINTER(ctypes.c_uint8) * 3
 LineSizes = ctypes.c_int64 * 3
+
+
+class SSIMU2BatchHandler(ctypes.Structure):
+    """Extension (include/VshipAPI_ext.h): handler of uneven SSIMULACRA2 batches."""
+    _fields_ = [("id", ctypes.c_uint)]
+
+
+class FramePair(ctypes.Structure):
+    """Extension (include/VshipAPI_ext.h): one pair of an uneven batch."""
+    _fields_ = [("src_colorspace", Colorspace), ("dis_colorspace", Colorspace),
+                ("srcp1", ctypes.c_void_p * 3), ("srcp2", ctypes.c_void_p * 3),
+                ("lineSize", ctypes.c_int64 * 3), ("lineSize2", ctypes.c_int64 * 3)]

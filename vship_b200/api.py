@@ -71,6 +71,19 @@ def _declare(L):
     L.VshipExt_ComputeSSIMU2NoAlloc.argtypes = [abi.Colorspace, abi.Colorspace, c.c_void_p, c.c_void_p, vpp, vpp,
                                                 i64p, i64p, c.c_void_p]
     L.VshipExt_ButteraugliResolution.argtypes = [HB, i64p, i64p]
+    HBt = abi.SSIMU2BatchHandler
+    FPp = c.POINTER(abi.FramePair)
+    L.VshipExt_SSIMU2BatchInit.argtypes = [c.POINTER(HBt), c.c_int]
+    L.VshipExt_SSIMU2BatchFree.argtypes = [HBt]
+    L.VshipExt_SSIMU2BatchGetDetailedLastError.argtypes = [HBt, c.c_char_p, c.c_int]
+    L.VshipExt_SSIMU2BatchGetDetailedLastError.restype = c.c_int
+    L.VshipExt_ComputeSSIMU2BatchDevice.argtypes = [HBt, c.c_int, FPp, c.c_void_p, c.c_void_p, c.c_void_p]
+    L.VshipExt_ComputeSSIMU2Batch.argtypes = [HBt, c.c_int, FPp, c.POINTER(c.c_double), c.c_void_p]
+    L.VshipExt_SSIMU2BatchSetTileRows.argtypes = [HBt, c.c_int]
+    L.VshipExt_SSIMU2BatchTileRows.argtypes = [HBt, c.POINTER(c.c_int)]
+    L.VshipExt_SSIMU2BatchKernelTiming.argtypes = [HBt, c.c_int]
+    L.VshipExt_SSIMU2BatchKernelTimes.argtypes = [HBt, c.c_void_p, c.c_int, c.c_int]
+    L.VshipExt_SSIMU2BatchKernelTimes.restype = c.c_int
     return L
 
 
@@ -272,6 +285,104 @@ class Butteraugli:
         if getattr(self, "alive", False):
             self.alive = False
             self.L.Vship_ButteraugliFree(self.h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def frame_pairs(items):
+    """FramePair array from (src_cs, dis_cs, planes1, planes2, line_sizes1, line_sizes2) tuples.
+
+    Planes are integer addresses (device or host) or numpy arrays (host); the returned
+    keep-alive list holds the arrays for as long as the pairs are used."""
+    arr = (abi.FramePair * len(items))()
+    keep = []
+    for i, (cs1, cs2, p1, p2, ls1, ls2) in enumerate(items):
+        fp = arr[i]
+        fp.src_colorspace, fp.dis_colorspace = cs1, cs2
+        for dst, planes in ((fp.srcp1, p1), (fp.srcp2, p2)):
+            for j, p in enumerate(planes):
+                if isinstance(p, int):
+                    dst[j] = p
+                else:
+                    keep.append(p)
+                    dst[j] = p.ctypes.data
+        for j in range(3):
+            fp.lineSize[j], fp.lineSize2[j] = ls1[j], ls2[j]
+    return arr, keep
+
+
+class SSIMU2Batch:
+    """Uneven SSIMULACRA2 batches (VshipExt_SSIMU2BatchInit .. VshipExt_SSIMU2BatchFree):
+    pairs of any resolutions and formats scored in one persistent launch."""
+
+    def __init__(self, gpu_id=0, lib=None):
+        self.L = lib or load()
+        self.h = abi.SSIMU2BatchHandler()
+        rc = self.L.VshipExt_SSIMU2BatchInit(ctypes.byref(self.h), gpu_id)
+        self.alive = True
+        if rc != 0:
+            msg = _message(self.L, self.L.VshipExt_SSIMU2BatchGetDetailedLastError, self.h)
+            self.close()
+            raise VshipError(rc, msg)
+
+    def _check(self, rc):
+        check(self.L, rc, self.L.VshipExt_SSIMU2BatchGetDetailedLastError, self.h)
+
+    def compute(self, pairs, features=False):
+        """Host-resident pairs (see frame_pairs); returns scores (and features (n, 108))."""
+        import numpy as np
+        arr, keep = frame_pairs(pairs)
+        n = len(pairs)
+        scores = np.zeros(n, dtype=np.float64)
+        feats = np.zeros((n, 108), dtype=np.float32) if features else None
+        self._check(self.L.VshipExt_ComputeSSIMU2Batch(
+            self.h, n, arr, scores.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            feats.ctypes.data if features else None))
+        return (scores, feats) if features else scores
+
+    def compute_device(self, pairs, d_scores, d_features=0, stream=0):
+        """Device-resident pairs (plane addresses are device pointers); asynchronous."""
+        arr, keep = frame_pairs(pairs)
+        self._check(self.L.VshipExt_ComputeSSIMU2BatchDevice(self.h, len(pairs), arr, d_scores,
+                                                              d_features or None, stream or None))
+
+    def compute_device_array(self, arr, n, d_scores, d_features=0, stream=0):
+        """As compute_device, with a prepared FramePair array (no per-call conversion)."""
+        self._check(self.L.VshipExt_ComputeSSIMU2BatchDevice(self.h, n, arr, d_scores, d_features or None,
+                                                              stream or None))
+
+    def set_tile_rows(self, rows):
+        self._check(self.L.VshipExt_SSIMU2BatchSetTileRows(self.h, int(rows)))
+
+    def tile_rows(self):
+        r = ctypes.c_int(0)
+        self._check(self.L.VshipExt_SSIMU2BatchTileRows(self.h, ctypes.byref(r)))
+        return r.value
+
+    def kernel_timing(self, enable=True):
+        self._check(self.L.VshipExt_SSIMU2BatchKernelTiming(self.h, 1 if enable else 0))
+
+    def kernel_times(self, reset=False):
+        out = (KernelTime * 8)()
+        n = self.L.VshipExt_SSIMU2BatchKernelTimes(self.h, out, 8, 1 if reset else 0)
+        if n < 0:
+            check(self.L, abi.BadHandler)
+        return {out[i].name.decode(): (out[i].launches, out[i].total_ms) for i in range(n)}
+
+    def close(self):
+        if getattr(self, "alive", False):
+            self.alive = False
+            self.L.VshipExt_SSIMU2BatchFree(self.h)
 
     def __enter__(self):
         return self

@@ -127,6 +127,7 @@ struct Table {
 
 Table<Ssimu2Api> g_ssimu2;
 Table<ButterApi> g_butter;
+Table<Ssimu2BatchApi> g_batch;
 
 template <typename EngineT>
 Vship_Exception fail(Slot<EngineT>* s, const Error& e) {
@@ -573,6 +574,73 @@ Vship_Exception VshipExt_ButteraugliResolution(Vship_ButteraugliHandler handler,
         if (width) *width = s.engine->width();
         if (height) *height = s.engine->height();
     });
+}
+
+// ---------------------------------------------------------------- uneven batches
+
+Vship_Exception VshipExt_SSIMU2BatchInit(VshipExt_SSIMU2BatchHandler* handler, int gpu_id) {
+    if (handler == nullptr) {
+        set_global_error(Error(Vship_BadPointer, __FILE__, __LINE__, "handler is NULL"));
+        return Vship_BadPointer;
+    }
+    return init_handler(g_batch, &handler->id, gpu_id, [&](Slot<Ssimu2BatchApi>& s) {
+        s.engine.reset(make_ssimu2_batch_engine());
+        s.engine->init(gpu_id);
+    });
+}
+
+Vship_Exception VshipExt_SSIMU2BatchFree(VshipExt_SSIMU2BatchHandler handler) {
+    return free_handler(g_batch, handler.id, "VshipExt_SSIMU2BatchFree");
+}
+
+int VshipExt_SSIMU2BatchGetDetailedLastError(VshipExt_SSIMU2BatchHandler handler, char* out_message, int len) {
+    return handler_error(g_batch, handler.id, out_message, len, "VshipExt_SSIMU2BatchGetDetailedLastError");
+}
+
+Vship_Exception VshipExt_ComputeSSIMU2BatchDevice(VshipExt_SSIMU2BatchHandler handler, int n, const VshipExt_FramePair* pairs,
+                                                  double* d_scores, float* d_features, void* stream) {
+    return with_handler(g_batch, handler.id, "VshipExt_ComputeSSIMU2BatchDevice", [&](Slot<Ssimu2BatchApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 0) throw Error(Vship_BadPointer, __FILE__, __LINE__, "negative pair count");
+        if (n > 0 && (!pairs || !d_scores)) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->compute_device(n, pairs, d_scores, d_features, (cudaStream_t)stream);
+    });
+}
+
+Vship_Exception VshipExt_ComputeSSIMU2Batch(VshipExt_SSIMU2BatchHandler handler, int n, const VshipExt_FramePair* pairs,
+                                            double* scores, float* features) {
+    return with_handler(g_batch, handler.id, "VshipExt_ComputeSSIMU2Batch", [&](Slot<Ssimu2BatchApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 0) throw Error(Vship_BadPointer, __FILE__, __LINE__, "negative pair count");
+        if (n > 0 && (!pairs || !scores)) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->compute(n, pairs, scores, features);
+    });
+}
+
+Vship_Exception VshipExt_SSIMU2BatchSetTileRows(VshipExt_SSIMU2BatchHandler handler, int rows) {
+    return with_handler(g_batch, handler.id, "VshipExt_SSIMU2BatchSetTileRows", [&](Slot<Ssimu2BatchApi>& s) {
+        require_engine((bool)s.engine);
+        s.engine->set_tile_rows(rows);
+    });
+}
+
+Vship_Exception VshipExt_SSIMU2BatchTileRows(VshipExt_SSIMU2BatchHandler handler, int* rows) {
+    return with_handler(g_batch, handler.id, "VshipExt_SSIMU2BatchTileRows", [&](Slot<Ssimu2BatchApi>& s) {
+        require_engine((bool)s.engine);
+        if (!rows) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        *rows = s.engine->tile_rows();
+    });
+}
+
+Vship_Exception VshipExt_SSIMU2BatchKernelTiming(VshipExt_SSIMU2BatchHandler handler, int enable) {
+    return with_handler(g_batch, handler.id, "VshipExt_SSIMU2BatchKernelTiming", [&](Slot<Ssimu2BatchApi>& s) {
+        require_engine((bool)s.engine);
+        s.engine->timer().enable(enable != 0);
+    });
+}
+
+int VshipExt_SSIMU2BatchKernelTimes(VshipExt_SSIMU2BatchHandler handler, VshipExt_KernelTime* out, int max, int reset) {
+    return kernel_times(g_batch, handler.id, out, max, reset);
 }
 
 }  // extern "C"

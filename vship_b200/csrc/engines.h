@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "common.cuh"
+#include "../../include/VshipAPI_ext.h"
 
 namespace vship {
 
@@ -44,7 +45,23 @@ struct ButterApi {
     virtual int height() const = 0;
 };
 
+// SSIMULACRA2 over uneven batches (no reference counterpart): pairs of any colourspaces in
+// one persistent launch replayed from a CUDA graph.
+struct Ssimu2BatchApi {
+    virtual ~Ssimu2BatchApi() = default;
+    virtual void init(int device) = 0;
+    // Device-resident pairs; asynchronous on `stream`.
+    virtual void compute_device(int n, const VshipExt_FramePair* pairs, double* d_scores, float* d_features,
+                                cudaStream_t stream) = 0;
+    // Host-resident pairs; blocks until scores (and features, when not null) are written.
+    virtual void compute(int n, const VshipExt_FramePair* pairs, double* scores, float* features) = 0;
+    virtual void set_tile_rows(int rows) = 0;
+    virtual int tile_rows() const = 0;
+    virtual KernelTimer& timer() = 0;
+};
+
 Ssimu2Api* make_ssimu2_engine();
+Ssimu2BatchApi* make_ssimu2_batch_engine();
 void record_global_error(const Error& e);
 ButterApi* make_butter_engine();
 

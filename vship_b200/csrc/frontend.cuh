@@ -134,45 +134,66 @@ struct StagingBuffer {
     }
 };
 
-// Copies the three host planes of one image to the device and returns the device view.
-// When the planes lie back to back in one host allocation (as FFVship lays out its pinned
-// frames), the whole frame goes in one copy and keeps the caller's strides; otherwise each
-// plane is copied densely.  Bytes past the last row of the last plane are never read (the
-// copy size follows src/gpuColorToLinear/vshipColor.hpp:96).
-inline RawImage stage_host_image(StagingBuffer& buf, const ClipGeometry& g, const uint8_t* const src[3],
-                                 const int64_t line_size[3], cudaStream_t stream) {
-    int64_t row[3];
+// Host planes of one image lie back to back in one allocation (as FFVship lays out its
+// pinned frames): the whole frame can go in one copy that keeps the caller's strides.
+inline bool contiguous_planes(const ClipGeometry& g, const uint8_t* const src[3], const int64_t line_size[3]) {
+    return src[1] == src[0] + line_size[0] * g.ph[0] && src[2] == src[1] + line_size[1] * g.ph[1];
+}
+
+// Device bytes copy_host_image() writes for these host planes (validates them).
+inline int64_t host_image_bytes(const ClipGeometry& g, const uint8_t* const src[3], const int64_t line_size[3]) {
     for (int c = 0; c < 3; c++) {
         if (src[c] == nullptr) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
-        row[c] = g.pw[c] * g.bytes;
-        if (line_size[c] < row[c]) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
+        if (line_size[c] < g.pw[c] * g.bytes) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
     }
+    if (contiguous_planes(g, src, line_size)) {
+        const int64_t bytes = line_size[0] * g.ph[0] + line_size[1] * g.ph[1] + line_size[2] * (g.ph[2] - 1) +
+                              g.pw[2] * g.bytes;
+        return round_up(bytes, 256);
+    }
+    int64_t off[3];
+    return dense_image_bytes(g, off);
+}
+
+// Copies the three host planes of one image to `dst` (host_image_bytes() bytes, 256-byte
+// aligned) and returns the device view.  Contiguous planes go in one copy and keep the
+// caller's strides; otherwise each plane is copied densely.  Bytes past the last row of the
+// last plane are never read (the copy size follows src/gpuColorToLinear/vshipColor.hpp:96).
+inline RawImage copy_host_image(uint8_t* dst, const ClipGeometry& g, const uint8_t* const src[3],
+                                const int64_t line_size[3], cudaStream_t stream) {
+    int64_t row[3];
+    for (int c = 0; c < 3; c++) row[c] = g.pw[c] * g.bytes;
     RawImage im;
-    const bool contiguous = src[1] == src[0] + line_size[0] * g.ph[0] && src[2] == src[1] + line_size[1] * g.ph[1];
-    if (contiguous) {
+    if (contiguous_planes(g, src, line_size)) {
         const int64_t bytes = line_size[0] * g.ph[0] + line_size[1] * g.ph[1] + line_size[2] * (g.ph[2] - 1) + row[2];
-        buf.ensure((size_t)round_up(bytes, 256), stream);
-        CUDA_CHECK(cudaMemcpyAsync(buf.ptr, src[0], (size_t)bytes, cudaMemcpyHostToDevice, stream));
+        CUDA_CHECK(cudaMemcpyAsync(dst, src[0], (size_t)bytes, cudaMemcpyHostToDevice, stream));
         for (int c = 0; c < 3; c++) {
-            im.p[c] = buf.ptr + (src[c] - src[0]);
+            im.p[c] = dst + (src[c] - src[0]);
             im.stride[c] = line_size[c];
         }
         return im;
     }
     int64_t off[3];
-    const int64_t total = dense_image_bytes(g, off);
-    buf.ensure((size_t)total, stream);
+    dense_image_bytes(g, off);
     for (int c = 0; c < 3; c++) {
-        im.p[c] = buf.ptr + off[c];
+        im.p[c] = dst + off[c];
         im.stride[c] = row[c];
         if (line_size[c] == row[c]) {
-            CUDA_CHECK(cudaMemcpyAsync(buf.ptr + off[c], src[c], (size_t)(row[c] * g.ph[c]), cudaMemcpyHostToDevice, stream));
+            CUDA_CHECK(cudaMemcpyAsync(dst + off[c], src[c], (size_t)(row[c] * g.ph[c]), cudaMemcpyHostToDevice, stream));
         } else {
-            CUDA_CHECK(cudaMemcpy2DAsync(buf.ptr + off[c], (size_t)row[c], src[c], (size_t)line_size[c], (size_t)row[c],
+            CUDA_CHECK(cudaMemcpy2DAsync(dst + off[c], (size_t)row[c], src[c], (size_t)line_size[c], (size_t)row[c],
                                          (size_t)g.ph[c], cudaMemcpyHostToDevice, stream));
         }
     }
     return im;
+}
+
+// Copies the three host planes of one image into a staging buffer (grown as needed) and
+// returns the device view.
+inline RawImage stage_host_image(StagingBuffer& buf, const ClipGeometry& g, const uint8_t* const src[3],
+                                 const int64_t line_size[3], cudaStream_t stream) {
+    buf.ensure((size_t)host_image_bytes(g, src, line_size), stream);
+    return copy_host_image(buf.ptr, g, src, line_size, stream);
 }
 
 // A stride that is not a multiple of the sample size makes the kernels use byte loads.
