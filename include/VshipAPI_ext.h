@@ -138,6 +138,53 @@ EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchKernelTiming(VshipExt_SSIMU
 EXPORTPREPROCESS int VshipExt_SSIMU2BatchKernelTimes(VshipExt_SSIMU2BatchHandler handler, VshipExt_KernelTime* out,
                                                      int max, int reset);
 
+/* ---- Learned surrogate ------------------------------------------------------------------
+ * No counterpart in the reference.  A small convolutional network predicts SSIMULACRA2 from
+ * the 1/8 and 1/16 XYB pyramid levels of both images (the coarse levels cost a fraction of
+ * the exact metric), for searches such as target-quality encoding that need many scores but
+ * only their side of a threshold: consult the prediction, and call the exact metric when it
+ * lands within a margin of the threshold.  A handler is bound to one colourspace pair (no
+ * resize or crop); its network runs at any resolution, so a model trained on one handler can
+ * be set on another.  Training, inference and gradients run on the library's own kernels. */
+typedef struct VshipExt_SurrogateHandler {
+    unsigned int id;
+} VshipExt_SurrogateHandler;
+
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateInit(VshipExt_SurrogateHandler* handler, Vship_Colorspace_t src_colorspace,
+                                                        Vship_Colorspace_t dis_colorspace, int gpu_id);
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateFree(VshipExt_SurrogateHandler handler);
+EXPORTPREPROCESS int VshipExt_SurrogateGetDetailedLastError(VshipExt_SurrogateHandler handler, char* out_message, int len);
+/* FP16 elements of one pair's network input. */
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateInputSize(VshipExt_SurrogateHandler handler, int64_t* elems);
+/* Network inputs of n device-resident pairs (3 plane pointers per image, as
+ * VshipExt_ComputeSSIMU2Device) into d_inputs (device, n * InputSize FP16), on `stream`. */
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateInputs(VshipExt_SurrogateHandler handler, int n,
+                                                          const uint8_t* const* srcp1, const uint8_t* const* srcp2,
+                                                          const int64_t lineSize[3], const int64_t lineSize2[3],
+                                                          void* d_inputs, void* stream);
+/* Predicted scores (device floats) of n prepared inputs, or of n device-resident pairs. */
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogatePredictInputs(VshipExt_SurrogateHandler handler, int n,
+                                                                 const void* d_inputs, float* d_pred, void* stream);
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogatePredict(VshipExt_SurrogateHandler handler, int n,
+                                                           const uint8_t* const* srcp1, const uint8_t* const* srcp2,
+                                                           const int64_t lineSize[3], const int64_t lineSize2[3],
+                                                           float* d_pred, void* stream);
+/* Trains the network from scratch (seeded) on n prepared inputs and their exact scores
+ * (device floats): Adam, cosine learning-rate decay from lr to lr / 20, MSE on the scores.
+ * loss_history (host, may be NULL) receives the mean loss of each epoch.  Synchronous. */
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateTrain(VshipExt_SurrogateHandler handler, int n, const void* d_inputs,
+                                                         const float* d_targets, int epochs, int batch, float lr,
+                                                         unsigned int seed, float* loss_history);
+/* Loss and its gradients (host floats, one per parameter) for the current model on n <= 1024
+ * prepared inputs; the model is not changed. */
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateGradients(VshipExt_SurrogateHandler handler, int n,
+                                                             const void* d_inputs, const float* d_targets, float* grads,
+                                                             double* loss);
+/* The model as floats (parameters, then the input normalisation): returns its length and
+ * fills `out` when max is at least that; -1 on error.  SetModel loads such a vector. */
+EXPORTPREPROCESS int VshipExt_SurrogateModel(VshipExt_SurrogateHandler handler, float* out, int max);
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateSetModel(VshipExt_SurrogateHandler handler, const float* model, int count);
+
 /* Metric resolution (after resize and crop) of a handler. */
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2Resolution(Vship_SSIMU2Handler handler, int64_t* width, int64_t* height);
 EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliResolution(Vship_ButteraugliHandler handler, int64_t* width, int64_t* height);

@@ -57,6 +57,7 @@ def lib():
                                          ctypes.c_int, dp, dp]
         L.oracle_blur.argtypes = [dp, dp, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_int]
         L.oracle_downsample.argtypes = [dp, ctypes.c_int64, ctypes.c_int64, dp]
+        L.oracle_positive_xyb.argtypes = [dp, ctypes.c_int64]
         L.oracle_num_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -121,6 +122,22 @@ def downsample(plane):
     out = np.empty(((h - 1) // 2 + 1, (w - 1) // 2 + 1), dtype=np.float64)
     lib().oracle_downsample(_dp(plane), w, h, _dp(out))
     return out
+
+
+def positive_xyb(rgb):
+    """Planar linear RGB (3, H, W) -> positive XYB (3, H, W), float64 (makeXYB.hpp:6-47)."""
+    out = np.array(rgb, dtype=np.float64, order="C", copy=True)
+    lib().oracle_positive_xyb(_dp(out), out.shape[1] * out.shape[2])
+    return out
+
+
+def pyramid_level(rgb, level):
+    """Linear RGB (3, H, W) -> positive XYB of pyramid level `level` (2x box downsamples of the
+    linear RGB, src/ssimu2/downsample.hpp:3-19, then XYB)."""
+    planes = [np.asarray(rgb[c], dtype=np.float64) for c in range(3)]
+    for _ in range(level):
+        planes = [downsample(p) for p in planes]
+    return positive_xyb(np.stack(planes))
 
 
 def num_threads():

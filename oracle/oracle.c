@@ -850,6 +850,17 @@ ORACLE_API void oracle_blur(const double* src, double* dst, int64_t w, int64_t h
 
 ORACLE_API void oracle_downsample(const double* src, int64_t w, int64_t h, double* dst) { downsample2(src, w, h, dst); }
 
+/* Planar linear RGB (3 planes of n samples) to positive XYB, in place. */
+ORACLE_API void oracle_positive_xyb(double* planes, int64_t n) {
+    for (int64_t i = 0; i < n; i++) {
+        double v[3] = {planes[i], planes[n + i], planes[2 * n + i]};
+        positive_xyb(v);
+        planes[i] = v[0];
+        planes[n + i] = v[1];
+        planes[2 * n + i] = v[2];
+    }
+}
+
 ORACLE_API int oracle_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -138,6 +138,11 @@ class SSIMU2BatchHandler(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint)]
 
 
+class SurrogateHandler(ctypes.Structure):
+    """Extension (include/VshipAPI_ext.h): handler of the learned SSIMULACRA2 surrogate."""
+    _fields_ = [("id", ctypes.c_uint)]
+
+
 class FramePair(ctypes.Structure):
     """Extension (include/VshipAPI_ext.h): one pair of an uneven batch."""
     _fields_ = [("src_colorspace", Colorspace), ("dis_colorspace", Colorspace),

@@ -84,6 +84,22 @@ def _declare(L):
     L.VshipExt_SSIMU2BatchKernelTiming.argtypes = [HBt, c.c_int]
     L.VshipExt_SSIMU2BatchKernelTimes.argtypes = [HBt, c.c_void_p, c.c_int, c.c_int]
     L.VshipExt_SSIMU2BatchKernelTimes.restype = c.c_int
+    HS = abi.SurrogateHandler
+    L.VshipExt_SurrogateInit.argtypes = [c.POINTER(HS), abi.Colorspace, abi.Colorspace, c.c_int]
+    L.VshipExt_SurrogateFree.argtypes = [HS]
+    L.VshipExt_SurrogateGetDetailedLastError.argtypes = [HS, c.c_char_p, c.c_int]
+    L.VshipExt_SurrogateGetDetailedLastError.restype = c.c_int
+    L.VshipExt_SurrogateInputSize.argtypes = [HS, i64p]
+    L.VshipExt_SurrogateInputs.argtypes = [HS, c.c_int, vpp, vpp, i64p, i64p, c.c_void_p, c.c_void_p]
+    L.VshipExt_SurrogatePredictInputs.argtypes = [HS, c.c_int, c.c_void_p, c.c_void_p, c.c_void_p]
+    L.VshipExt_SurrogatePredict.argtypes = [HS, c.c_int, vpp, vpp, i64p, i64p, c.c_void_p, c.c_void_p]
+    L.VshipExt_SurrogateTrain.argtypes = [HS, c.c_int, c.c_void_p, c.c_void_p, c.c_int, c.c_int, c.c_float, c.c_uint,
+                                          c.c_void_p]
+    L.VshipExt_SurrogateGradients.argtypes = [HS, c.c_int, c.c_void_p, c.c_void_p, c.c_void_p,
+                                              c.POINTER(c.c_double)]
+    L.VshipExt_SurrogateModel.argtypes = [HS, c.c_void_p, c.c_int]
+    L.VshipExt_SurrogateModel.restype = c.c_int
+    L.VshipExt_SurrogateSetModel.argtypes = [HS, c.c_void_p, c.c_int]
     return L
 
 
@@ -383,6 +399,94 @@ class SSIMU2Batch:
         if getattr(self, "alive", False):
             self.alive = False
             self.L.VshipExt_SSIMU2BatchFree(self.h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Surrogate:
+    """The learned SSIMULACRA2 surrogate of one colourspace pair (VshipExt_Surrogate*).
+
+    Device arrays are passed as integer addresses (e.g. torch `data_ptr()`)."""
+
+    def __init__(self, src_cs, dis_cs=None, gpu_id=0, lib=None):
+        self.L = lib or load()
+        self.h = abi.SurrogateHandler()
+        rc = self.L.VshipExt_SurrogateInit(ctypes.byref(self.h), src_cs, dis_cs or src_cs, gpu_id)
+        self.alive = True
+        if rc != 0:
+            msg = _message(self.L, self.L.VshipExt_SurrogateGetDetailedLastError, self.h)
+            self.close()
+            raise VshipError(rc, msg)
+
+    def _check(self, rc):
+        check(self.L, rc, self.L.VshipExt_SurrogateGetDetailedLastError, self.h)
+
+    def input_elems(self):
+        n = ctypes.c_int64(0)
+        self._check(self.L.VshipExt_SurrogateInputSize(self.h, ctypes.byref(n)))
+        return n.value
+
+    def inputs(self, n, ptrs1, ptrs2, line_sizes1, line_sizes2, d_inputs, stream=0):
+        a1 = (ctypes.c_void_p * (3 * n))(*ptrs1)
+        a2 = (ctypes.c_void_p * (3 * n))(*ptrs2)
+        self._check(self.L.VshipExt_SurrogateInputs(self.h, n, a1, a2, abi.LineSizes(*line_sizes1),
+                                                    abi.LineSizes(*line_sizes2), d_inputs, stream or None))
+
+    def predict(self, n, ptrs1, ptrs2, line_sizes1, line_sizes2, d_pred, stream=0):
+        a1 = (ctypes.c_void_p * (3 * n))(*ptrs1)
+        a2 = (ctypes.c_void_p * (3 * n))(*ptrs2)
+        self._check(self.L.VshipExt_SurrogatePredict(self.h, n, a1, a2, abi.LineSizes(*line_sizes1),
+                                                     abi.LineSizes(*line_sizes2), d_pred, stream or None))
+
+    def predict_inputs(self, n, d_inputs, d_pred, stream=0):
+        self._check(self.L.VshipExt_SurrogatePredictInputs(self.h, n, d_inputs, d_pred, stream or None))
+
+    def train(self, n, d_inputs, d_targets, epochs=8, batch=256, lr=3e-3, seed=1):
+        import numpy as np
+        hist = np.zeros(epochs, dtype=np.float32)
+        self._check(self.L.VshipExt_SurrogateTrain(self.h, n, d_inputs, d_targets, epochs, batch, lr, seed,
+                                                   hist.ctypes.data))
+        return hist
+
+    def gradients(self, n, d_inputs, d_targets):
+        import numpy as np
+        g = np.zeros(self.num_params(), dtype=np.float32)
+        loss = ctypes.c_double()
+        self._check(self.L.VshipExt_SurrogateGradients(self.h, n, d_inputs, d_targets, g.ctypes.data,
+                                                       ctypes.byref(loss)))
+        return loss.value, g
+
+    def model(self):
+        import numpy as np
+        n = self.L.VshipExt_SurrogateModel(self.h, None, 0)
+        if n < 0:
+            self._check(abi.BadHandler)
+        out = np.zeros(n, dtype=np.float32)
+        self.L.VshipExt_SurrogateModel(self.h, out.ctypes.data, n)
+        return out
+
+    def num_params(self):
+        return self.L.VshipExt_SurrogateModel(self.h, None, 0) - 12
+
+    def set_model(self, model):
+        import numpy as np
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        self._check(self.L.VshipExt_SurrogateSetModel(self.h, m.ctypes.data, len(m)))
+
+    def close(self):
+        if getattr(self, "alive", False):
+            self.alive = False
+            self.L.VshipExt_SurrogateFree(self.h)
 
     def __enter__(self):
         return self

@@ -128,6 +128,7 @@ struct Table {
 Table<Ssimu2Api> g_ssimu2;
 Table<ButterApi> g_butter;
 Table<Ssimu2BatchApi> g_batch;
+Table<SurrogateApi> g_surrogate;
 
 template <typename EngineT>
 Vship_Exception fail(Slot<EngineT>* s, const Error& e) {
@@ -641,6 +642,107 @@ Vship_Exception VshipExt_SSIMU2BatchKernelTiming(VshipExt_SSIMU2BatchHandler han
 
 int VshipExt_SSIMU2BatchKernelTimes(VshipExt_SSIMU2BatchHandler handler, VshipExt_KernelTime* out, int max, int reset) {
     return kernel_times(g_batch, handler.id, out, max, reset);
+}
+
+// ---------------------------------------------------------------- learned surrogate
+
+Vship_Exception VshipExt_SurrogateInit(VshipExt_SurrogateHandler* handler, Vship_Colorspace_t src, Vship_Colorspace_t dis,
+                                       int gpu_id) {
+    if (handler == nullptr) {
+        set_global_error(Error(Vship_BadPointer, __FILE__, __LINE__, "handler is NULL"));
+        return Vship_BadPointer;
+    }
+    return init_handler(g_surrogate, &handler->id, gpu_id, [&](Slot<SurrogateApi>& s) {
+        s.engine.reset(make_surrogate_engine());
+        s.engine->init(src, dis, gpu_id);
+    });
+}
+
+Vship_Exception VshipExt_SurrogateFree(VshipExt_SurrogateHandler handler) {
+    return free_handler(g_surrogate, handler.id, "VshipExt_SurrogateFree");
+}
+
+int VshipExt_SurrogateGetDetailedLastError(VshipExt_SurrogateHandler handler, char* out_message, int len) {
+    return handler_error(g_surrogate, handler.id, out_message, len, "VshipExt_SurrogateGetDetailedLastError");
+}
+
+Vship_Exception VshipExt_SurrogateInputSize(VshipExt_SurrogateHandler handler, int64_t* elems) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateInputSize", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (!elems) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        *elems = s.engine->input_elems();
+    });
+}
+
+Vship_Exception VshipExt_SurrogateInputs(VshipExt_SurrogateHandler handler, int n, const uint8_t* const* srcp1,
+                                         const uint8_t* const* srcp2, const int64_t lineSize[3], const int64_t lineSize2[3],
+                                         void* d_inputs, void* stream) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateInputs", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 0) throw Error(Vship_BadPointer, __FILE__, __LINE__, "negative pair count");
+        if (n > 0 && (!srcp1 || !srcp2 || !lineSize || !lineSize2 || !d_inputs))
+            throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->inputs(n, srcp1, srcp2, lineSize, lineSize2, d_inputs, (cudaStream_t)stream);
+    });
+}
+
+Vship_Exception VshipExt_SurrogatePredictInputs(VshipExt_SurrogateHandler handler, int n, const void* d_inputs,
+                                                float* d_pred, void* stream) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogatePredictInputs", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 0) throw Error(Vship_BadPointer, __FILE__, __LINE__, "negative sample count");
+        if (n > 0 && (!d_inputs || !d_pred)) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->predict_inputs(n, d_inputs, d_pred, (cudaStream_t)stream);
+    });
+}
+
+Vship_Exception VshipExt_SurrogatePredict(VshipExt_SurrogateHandler handler, int n, const uint8_t* const* srcp1,
+                                          const uint8_t* const* srcp2, const int64_t lineSize[3],
+                                          const int64_t lineSize2[3], float* d_pred, void* stream) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogatePredict", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 0) throw Error(Vship_BadPointer, __FILE__, __LINE__, "negative pair count");
+        if (n > 0 && (!srcp1 || !srcp2 || !lineSize || !lineSize2 || !d_pred))
+            throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->predict(n, srcp1, srcp2, lineSize, lineSize2, d_pred, (cudaStream_t)stream);
+    });
+}
+
+Vship_Exception VshipExt_SurrogateTrain(VshipExt_SurrogateHandler handler, int n, const void* d_inputs,
+                                        const float* d_targets, int epochs, int batch, float lr, unsigned seed,
+                                        float* loss_history) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateTrain", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (!d_inputs || !d_targets) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->train(n, d_inputs, d_targets, epochs, batch, lr, seed, loss_history);
+    });
+}
+
+Vship_Exception VshipExt_SurrogateGradients(VshipExt_SurrogateHandler handler, int n, const void* d_inputs,
+                                            const float* d_targets, float* grads, double* loss) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateGradients", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 1 || !d_inputs || !d_targets) throw Error(Vship_BadPointer, __FILE__, __LINE__, "bad argument");
+        const double l = s.engine->gradients(n, d_inputs, d_targets, grads);
+        if (loss) *loss = l;
+    });
+}
+
+int VshipExt_SurrogateModel(VshipExt_SurrogateHandler handler, float* out, int max) {
+    int count = -1;
+    Vship_Exception rc = with_handler(g_surrogate, handler.id, "VshipExt_SurrogateModel", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        count = s.engine->get_model(out, max);
+    });
+    return rc == Vship_NoError ? count : -1;
+}
+
+Vship_Exception VshipExt_SurrogateSetModel(VshipExt_SurrogateHandler handler, const float* model, int count) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateSetModel", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (!model) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->set_model(model, count);
+    });
 }
 
 }  // extern "C"

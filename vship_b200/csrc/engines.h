@@ -60,7 +60,31 @@ struct Ssimu2BatchApi {
     virtual KernelTimer& timer() = 0;
 };
 
+// Learned SSIMULACRA2 surrogate bound to one colourspace pair (no reference counterpart).
+struct SurrogateApi {
+    virtual ~SurrogateApi() = default;
+    virtual void init(const Vship_Colorspace_t& src, const Vship_Colorspace_t& dis, int device) = 0;
+    virtual int64_t input_elems() const = 0;   // FP16 elements of one pair's network input
+    virtual int num_params() const = 0;
+    // Network inputs of n device-resident pairs into d_inputs (n * input_elems() FP16).
+    virtual void inputs(int n, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t ls1[3],
+                        const int64_t ls2[3], void* d_inputs, cudaStream_t stream) = 0;
+    virtual void predict_inputs(int n, const void* d_inputs, float* d_pred, cudaStream_t stream) = 0;
+    // Inputs and predictions of n device-resident pairs (internal input buffer).
+    virtual void predict(int n, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t ls1[3],
+                         const int64_t ls2[3], float* d_pred, cudaStream_t stream) = 0;
+    // Loss and gradients (FP32, num_params()) of the current weights on n samples.
+    virtual double gradients(int n, const void* d_inputs, const float* d_targets, float* grads_host) = 0;
+    virtual void train(int n, const void* d_inputs, const float* d_targets, int epochs, int batch, float lr,
+                       unsigned seed, float* loss_history) = 0;
+    // Model = parameters then input normalisation (shift[6], scale[6]); returns its length.
+    virtual int get_model(float* out, int max) = 0;
+    virtual void set_model(const float* in, int count) = 0;
+    virtual KernelTimer& timer() = 0;
+};
+
 Ssimu2Api* make_ssimu2_engine();
+SurrogateApi* make_surrogate_engine();
 Ssimu2BatchApi* make_ssimu2_batch_engine();
 void record_global_error(const Error& e);
 ButterApi* make_butter_engine();

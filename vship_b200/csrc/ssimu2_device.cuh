@@ -78,7 +78,7 @@ struct LevelTile {
 // Builds level L (tile size T) of tile (tx, ty) from level L-1 held in `src` (tile size 2T),
 // writes its XYB planes, keeps its linear RGB in `dst`.  Downsample order and clamps follow
 // src/ssimu2/downsample.hpp:3-19.
-template <int T>
+template <int T, bool kXyb = true>
 __device__ __forceinline__ void build_level(const LevelTile<2 * T>& src, LevelTile<T>& dst, int L,
                                             const Pyramid& pyr, float* img_out, int tx, int ty) {
     const int W = pyr.w[L], H = pyr.h[L], Wp = pyr.w[L - 1], Hp = pyr.h[L - 1];
@@ -101,11 +101,13 @@ __device__ __forceinline__ void build_level(const LevelTile<2 * T>& src, LevelTi
             dp[c] = t;
             dst.v[c][ly][lx] = t;
         }
-        const float3 q = positive_xyb(d);
-        const float qv[3] = {q.x, q.y, q.z};
+        if (kXyb) {
+            const float3 q = positive_xyb(d);
+            const float qv[3] = {q.x, q.y, q.z};
 #pragma unroll
-        for (int p = 0; p < 3; p++)
-            if (pyr.off[L][p] >= 0) img_out[pyr.off[L][p] + (int64_t)gy * pyr.pitch[L] + gx] = qv[p];
+            for (int p = 0; p < 3; p++)
+                if (pyr.off[L][p] >= 0) img_out[pyr.off[L][p] + (int64_t)gy * pyr.pitch[L] + gx] = qv[p];
+        }
     }
 }
 
@@ -128,8 +130,9 @@ struct LinearIn {
 // One front tile: level-0 pixels [64 tx, 64 tx + 64) x [64 ty, 64 ty + 64) of one image to
 // linear RGB, levels 1-5 of the tile in shared memory, and every stored XYB plane of the
 // tile written to `out` (the image's pyramid).  `stage_mem` holds the chroma stage when the
-// clip is subsampled.  Ends after the last level is written (no trailing barrier).
-template <bool FromLinear, int kFast>
+// clip is subsampled.  kCoarse computes XYB at levels 3 and 4 only (the inputs of the
+// learned surrogate).  Ends after the last level is written (no trailing barrier).
+template <bool FromLinear, int kFast, bool kCoarse = false>
 __device__ __forceinline__ void front_tile(FrontSmem& fs, float* stage_mem, const ColourParams& cp,
                                            const RawImage& im, const LinearIn& lin, const Pyramid& pyr,
                                            float* out, int tx, int ty) {
@@ -164,6 +167,7 @@ __device__ __forceinline__ void front_tile(FrontSmem& fs, float* stage_mem, cons
         const float3 p10 = (Y1 != Y0) ? pixel(X0, Y1) : p00;
         const float3 p11 = (Y1 != Y0) ? ((X1 != X0) ? pixel(X1, Y1) : p10) : p01;
         // Level-0 XYB: only the Y plane has unpruned maps at full resolution.
+        if (!kCoarse) {
         const float y00 = positive_xyb(p00).y;
         if (X1 != X0) {
             *reinterpret_cast<float2*>(y0plane + (int64_t)Y0 * pitch0 + X0) = make_float2(y00, positive_xyb(p01).y);
@@ -174,6 +178,7 @@ __device__ __forceinline__ void front_tile(FrontSmem& fs, float* stage_mem, cons
             y0plane[(int64_t)Y0 * pitch0 + X0] = y00;
             if (Y1 != Y0) y0plane[(int64_t)Y1 * pitch0 + X0] = positive_xyb(p10).y;
         }
+        }
         float3 d;
         d.x = p00.x; d.x += p10.x; d.x += p01.x; d.x += p11.x; d.x *= 0.25f;
         d.y = p00.y; d.y += p10.y; d.y += p01.y; d.y += p11.y; d.y *= 0.25f;
@@ -181,20 +186,24 @@ __device__ __forceinline__ void front_tile(FrontSmem& fs, float* stage_mem, cons
         fs.t1.v[0][qy][qx] = d.x;
         fs.t1.v[1][qy][qx] = d.y;
         fs.t1.v[2][qy][qx] = d.z;
-        const float3 x1 = positive_xyb(d);
-        const float xv[3] = {x1.x, x1.y, x1.z};
+        if (!kCoarse) {
+            const float3 x1 = positive_xyb(d);
+            const float xv[3] = {x1.x, x1.y, x1.z};
 #pragma unroll
-        for (int p = 0; p < 3; p++)
-            if (pyr.off[1][p] >= 0) out[pyr.off[1][p] + (int64_t)gy * pyr.pitch[1] + gx] = xv[p];
+            for (int p = 0; p < 3; p++)
+                if (pyr.off[1][p] >= 0) out[pyr.off[1][p] + (int64_t)gy * pyr.pitch[1] + gx] = xv[p];
+        }
     }
     __syncthreads();
-    build_level<16>(fs.t1, fs.t2, 2, pyr, out, tx, ty);
+    build_level<16, !kCoarse>(fs.t1, fs.t2, 2, pyr, out, tx, ty);
     __syncthreads();
     build_level<8>(fs.t2, fs.t3, 3, pyr, out, tx, ty);
     __syncthreads();
     build_level<4>(fs.t3, fs.t4, 4, pyr, out, tx, ty);
-    __syncthreads();
-    build_level<2>(fs.t4, fs.t5, 5, pyr, out, tx, ty);
+    if (!kCoarse) {
+        __syncthreads();
+        build_level<2>(fs.t4, fs.t5, 5, pyr, out, tx, ty);
+    }
 }
 
 constexpr int kTile = 32;
