@@ -731,6 +731,129 @@ def run_uneven_reference(args, world, rank, local):
         flush=True)
 
 
+SWORKLOAD = "surrogate_target_quality_train200k_512_eval1000_1080p_yuv420p10"
+SMETRIC = "surrogate target-quality search: exact SSIMU2 calls saved"
+
+
+def run_surrogate(args, world, rank, local):
+    """Learned surrogate, end to end: a training set of seeded 512x512 10-bit 4:2:0 pairs (DCT
+    steps uniform in [2, 64]) scored by the exact engine, training on the GPU with the
+    library's own kernels, then bisection to SSIMULACRA2 = 80 over 1080p frames with the
+    surrogate (exact fallback within +/-2) and without it."""
+    import torch
+    from vship_b200 import abi, api, target_quality as tq
+    torch.cuda.set_device(local)
+    out = {"metric": SMETRIC, "unit": "fraction of exact calls saved", "n_gpus": 1, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP16 weights)", "data": "synthetic"}
+    cs512 = abi.yuv420_10bit_bt709(512, 512)
+    sur = api.Surrogate(cs512)
+    ex512 = api.SSIMU2(cs512)
+    n, held = args.sur_train, 4096
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    X, T = tq.build_training_set(sur, ex512, n + held, 512, 512, seed=2024, chunk=1024)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    hist = sur.train(n, X.data_ptr(), T.data_ptr(), epochs=args.sur_epochs, batch=256, lr=3e-3, seed=11)
+    t2 = time.perf_counter()
+    pred = torch.zeros(held, dtype=torch.float32, device="cuda")
+    sur.predict_inputs(held, X[n].data_ptr(), pred.data_ptr())
+    torch.cuda.synchronize()
+    tgt = T[n:].cpu().numpy()
+    rmse512 = tq.rmse(pred.cpu().numpy(), tgt)
+    model = sur.model()
+    ex512.close()
+    sur.close()
+    del X, T
+    torch.cuda.empty_cache()
+    log("training set %d pairs in %.1fs, training %d epochs in %.1fs, held-out RMSE %.3f (std %.2f)"
+        % (n + held, t1 - t0, args.sur_epochs, t2 - t1, rmse512, tgt.std()))
+
+    # Bisection over 1080p frames.
+    w, h, frames = 1920, 1080, args.sur_frames
+    cs = abi.yuv420_10bit_bt709(w, h)
+    sur = api.Surrogate(cs)
+    sur.set_model(model)
+    ex = api.SSIMU2(cs)
+    gen = tq.GpuFrames()
+    refs = torch.empty((frames, 3, h, w), dtype=torch.uint8, device="cuda")
+    for i0 in range(0, frames, 32):
+        i1 = min(frames, i0 + 32)
+        refs[i0:i1] = gen.references(i1 - i0, w, h, seed=500 + i0).round().to(torch.uint8)
+    ref_yuv = [torch.empty((frames, h, w), dtype=torch.int16, device="cuda"),
+               torch.empty((frames, h // 2, w // 2), dtype=torch.int16, device="cuda"),
+               torch.empty((frames, h // 2, w // 2), dtype=torch.int16, device="cuda")]
+    for i0 in range(0, frames, 32):
+        i1 = min(frames, i0 + 32)
+        for dst, src in zip(ref_yuv, gen.yuv420p10(refs[i0:i1].float())):
+            dst[i0:i1] = src
+
+    def fy(i0, i1):
+        return tuple(x[i0:i1] for x in ref_yuv)
+
+    def dy(i0, i1, st):
+        return gen.yuv420p10(gen.dct_quantize(refs[i0:i1].float(), st))
+
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    base = tq.search(fy, dy, frames, ex, None)
+    torch.cuda.synchronize()
+    t4 = time.perf_counter()
+    guided = tq.search(fy, dy, frames, ex, sur)
+    torch.cuda.synchronize()
+    t5 = time.perf_counter()
+    fa = tq.final_scores(fy, dy, frames, ex, base["step"])
+    fb = tq.final_scores(fy, dy, frames, ex, guided["step"])
+
+    # Cost of one prediction against one exact score (device-resident 1080p pairs, 64 per call).
+    yb = dy(0, 64, np.full(64, 20.0))
+    p1, ls = tq.planes_of(fy(0, 64))
+    p2, _ = tq.planes_of(yb)
+    pr = torch.zeros(64, dtype=torch.float32, device="cuda")
+    sc = torch.zeros(64, dtype=torch.float64, device="cuda")
+
+    def rate(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return 64 * reps / (e0.elapsed_time(e1) / 1e3)
+
+    sur_rate = rate(lambda: sur.predict(64, p1, p2, ls, ls, pr.data_ptr()))
+    ex_rate = rate(lambda: ex.compute_device(64, p1, p2, ls, ls, sc.data_ptr(), 0, 0))
+    sur.close()
+    ex.close()
+    saved = 1.0 - guided["exact_calls"] / base["exact_calls"]
+    errs = np.array(guided["surrogate_errors"])
+    out.update({
+        "value": round(saved, 4), "steps": 1, "warmup": 0,
+        "config": {"workload": SWORKLOAD, "train_pairs": n, "train_size": "512x512", "held_out": held,
+                   "eval_frames": frames, "eval_size": "1920x1080", "format": "YUV420 10-bit limited BT.709",
+                   "target": 80.0, "margin": 2.0, "bisection": "7 halvings of step in [2, 64]",
+                   "epochs": args.sur_epochs, "batch": 256},
+        "exact_calls": {"with_surrogate": guided["exact_calls"], "without": base["exact_calls"],
+                        "probes": guided["probes"]},
+        "final_abs_error": {"with_surrogate": round(float(np.mean(np.abs(fb - 80))), 4),
+                            "without": round(float(np.mean(np.abs(fa - 80))), 4),
+                            "max_with_surrogate": round(float(np.max(np.abs(fb - 80))), 4)},
+        "same_decision_fraction": round(float(np.mean(np.abs(base["step"] - guided["step"]) < 1e-9)), 4),
+        "mean_abs_step_difference": round(float(np.mean(np.abs(base["step"] - guided["step"]))), 4),
+        "surrogate_rmse": {"held_out_512": round(rmse512, 4), "held_out_std": round(float(tgt.std()), 3),
+                           "near_threshold_1080p_mae": round(float(errs.mean()), 4) if len(errs) else None},
+        "training": {"set_seconds": round(t1 - t0, 2), "train_seconds": round(t2 - t1, 2),
+                     "samples_per_second": round(n * args.sur_epochs / (t2 - t1), 1),
+                     "loss_per_epoch": [round(float(x), 5) for x in hist]},
+        "search_seconds": {"without": round(t4 - t3, 2), "with_surrogate": round(t5 - t4, 2)},
+        "pairs_per_second_1080p": {"surrogate": round(sur_rate, 1), "exact": round(ex_rate, 1)},
+    })
+    print(json.dumps(out), flush=True)
+
+
 def run_profile_case(args):
     """Small device-resident run for ncu captures: `--profile-pairs` 1080p pairs, `--steps`
     calls of VshipExt_ComputeSSIMU2Device, nothing else (no timing, no e2e, no CPU leg)."""
@@ -801,10 +924,13 @@ def main():
     ap.add_argument("--ref-threads", type=int, nargs="+", default=[1, 3, 4, 8])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli", "ssimu2-uneven"],
+    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli", "ssimu2-uneven", "surrogate"],
                     help="butteraugli: secondary 4K Butteraugli line; ssimu2-uneven: 256 pairs of mixed "
                          "resolutions in one persistent launch, instead of the headline metric")
     ap.add_argument("--tile-rows", type=int, default=0, help="ssimu2-uneven: fixed map tile rows (0: autotune)")
+    ap.add_argument("--sur-train", type=int, default=200000, help="surrogate: training pairs")
+    ap.add_argument("--sur-epochs", type=int, default=8, help="surrogate: training epochs")
+    ap.add_argument("--sur-frames", type=int, default=1000, help="surrogate: 1080p frames searched")
     ap.add_argument("--profile-pairs", type=int, default=0,
                     help="only run N device-resident pairs --steps times (for ncu captures)")
     ap.add_argument("--profile-uneven", type=int, default=0,
@@ -823,6 +949,14 @@ def main():
     if args.metric == "butteraugli":
         if args.impl == "ours" and rank == 0:
             run_butteraugli(args, world, rank, local)
+        return
+    if args.metric == "surrogate":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no surrogate or "
+                                  "target-quality search; its exact metric is measured by the other metrics"}))
+        elif rank == 0:
+            run_surrogate(args, world, rank, local)
         return
     if args.metric == "ssimu2-uneven":
         if args.impl == "reference":
