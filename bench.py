@@ -824,7 +824,10 @@ def run_surrogate(args, world, rank, local):
         torch.cuda.synchronize()
         return 64 * reps / (e0.elapsed_time(e1) / 1e3)
 
+    refs64 = torch.zeros((64, sur.reference_floats()), dtype=torch.float32, device="cuda")
+    sur.references(64, p1, ls, refs64.data_ptr())
     sur_rate = rate(lambda: sur.predict(64, p1, p2, ls, ls, pr.data_ptr()))
+    against_rate = rate(lambda: sur.predict_against(64, refs64.data_ptr(), p2, ls, pr.data_ptr()))
     ex_rate = rate(lambda: ex.compute_device(64, p1, p2, ls, ls, sc.data_ptr(), 0, 0))
     sur.close()
     ex.close()
@@ -849,7 +852,13 @@ def run_surrogate(args, world, rank, local):
                      "samples_per_second": round(n * args.sur_epochs / (t2 - t1), 1),
                      "loss_per_epoch": [round(float(x), 5) for x in hist]},
         "search_seconds": {"without": round(t4 - t3, 2), "with_surrogate": round(t5 - t4, 2)},
-        "pairs_per_second_1080p": {"surrogate": round(sur_rate, 1), "exact": round(ex_rate, 1)},
+        "pairs_per_second_1080p": {"surrogate_pair": round(sur_rate, 1),
+                                   "surrogate_against_prepared_reference": round(against_rate, 1),
+                                   "exact": round(ex_rate, 1)},
+        "search_gpu_ms_estimate": {
+            "without": round(base["exact_calls"] / ex_rate * 1e3, 1),
+            "with_surrogate": round((guided["probes"] / against_rate + guided["exact_calls"] / ex_rate
+                                     + frames / (2 * against_rate)) * 1e3, 1)},
     })
     print(json.dumps(out), flush=True)
 
@@ -914,6 +923,27 @@ def run_profile_uneven(args):
         (n, float(np.max(np.abs(scores.cpu().numpy() - batch)))))
 
 
+def run_profile_butter(args):
+    """Small device-resident Butteraugli run for ncu captures: `--profile-butter` 4K 8-bit sRGB
+    pairs (intensity 203, Q-norm 5, distortion map on), `--steps` calls each, nothing else."""
+    import torch
+    from vship_b200 import abi, api, synth
+    n = args.profile_butter
+    pairs = synth.make_pairs(n, BW, BH, fmt="rgb8", seed=77, unique=1, blur=(0.0, 1.5))
+    cs = abi.srgb8(BW, BH)
+    ls = pairs[0][2]
+    dev = [([torch.from_numpy(p).cuda() for p in a], [torch.from_numpy(p).cuda() for p in b]) for a, b, _ in pairs]
+    norms = torch.zeros(n, 3, dtype=torch.float64, device="cuda")
+    dmap = torch.zeros(BH, BW, dtype=torch.float32, device="cuda")
+    with api.Butteraugli(cs, qnorm=5, intensity=203.0) as h:
+        for _ in range(args.steps):
+            for i, (d1, d2) in enumerate(dev):
+                h.compute_device([x.data_ptr() for x in d1], [x.data_ptr() for x in d2], ls, ls,
+                                 norms[i].data_ptr(), dmap.data_ptr(), BW * 4, 0)
+        torch.cuda.synchronize()
+    log("profile butteraugli: %d pairs x %d calls, norms %s" % (n, args.steps, np.round(norms.cpu().numpy()[0], 4)))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -933,6 +963,8 @@ def main():
     ap.add_argument("--sur-frames", type=int, default=1000, help="surrogate: 1080p frames searched")
     ap.add_argument("--profile-pairs", type=int, default=0,
                     help="only run N device-resident pairs --steps times (for ncu captures)")
+    ap.add_argument("--profile-butter", type=int, default=0,
+                    help="only run N 4K Butteraugli pairs --steps times (for ncu captures)")
     ap.add_argument("--profile-uneven", type=int, default=0,
                     help="only run N uneven pairs through the batch graph --steps times and once per "
                          "resolution through handlers (for ncu captures)")
@@ -942,6 +974,9 @@ def main():
         return
     if args.profile_uneven:
         run_profile_uneven(args)
+        return
+    if args.profile_butter:
+        run_profile_butter(args)
         return
     if args.warmup < 3:
         args.warmup = 3

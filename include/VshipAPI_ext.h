@@ -169,6 +169,17 @@ EXPORTPREPROCESS Vship_Exception VshipExt_SurrogatePredict(VshipExt_SurrogateHan
                                                            const uint8_t* const* srcp1, const uint8_t* const* srcp2,
                                                            const int64_t lineSize[3], const int64_t lineSize2[3],
                                                            float* d_pred, void* stream);
+/* Searches probe one reference frame against many distortions of it: prepare the references'
+ * coarse levels once (device floats, ReferenceSize each, n references back to back), then
+ * predict distorted frames against them (pair i uses reference i); the predictions equal
+ * those of VshipExt_SurrogatePredict on the same pairs, at about half the cost. */
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateReferenceSize(VshipExt_SurrogateHandler handler, int64_t* floats);
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateReferences(VshipExt_SurrogateHandler handler, int n,
+                                                              const uint8_t* const* srcp1, const int64_t lineSize[3],
+                                                              float* d_refs, void* stream);
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogatePredictAgainst(VshipExt_SurrogateHandler handler, int n,
+                                                                  const float* d_refs, const uint8_t* const* srcp2,
+                                                                  const int64_t lineSize2[3], float* d_pred, void* stream);
 /* Trains the network from scratch (seeded) on n prepared inputs and their exact scores
  * (device floats): Adam, cosine learning-rate decay from lr to lr / 20, MSE on the scores.
  * loss_history (host, may be NULL) receives the mean loss of each epoch.  Synchronous. */

@@ -121,6 +121,28 @@ def test_coarse_inputs_match_oracle_levels(gpu, oracle_lib):
             np.testing.assert_allclose(lv[3:], xb - xa, rtol=2e-3, atol=2e-5)  # FP16 of small differences
 
 
+def test_predictions_against_prepared_references_equal_pair_predictions(gpu):
+    import torch
+    cs = abi.yuv420_10bit_bt709(W, H)
+    pairs = synth.make_pairs(5, W, H, fmt="yuv420p10", seed=21)
+    with api.Surrogate(cs) as sur:
+        params, norm = _random_model(13)
+        sur.set_model(np.concatenate([params, norm]))
+        dev = [([torch.from_numpy(p.view(np.uint8).copy()).cuda() for p in a],
+                [torch.from_numpy(p.view(np.uint8).copy()).cuda() for p in b]) for a, b, _ in pairs]
+        ls = pairs[0][2]
+        p1 = [t.data_ptr() for d in dev for t in d[0]]
+        p2 = [t.data_ptr() for d in dev for t in d[1]]
+        direct = torch.zeros(5, dtype=torch.float32, device="cuda")
+        sur.predict(5, p1, p2, ls, ls, direct.data_ptr())
+        refs = torch.zeros((5, sur.reference_floats()), dtype=torch.float32, device="cuda")
+        sur.references(5, p1, ls, refs.data_ptr())
+        against = torch.zeros(5, dtype=torch.float32, device="cuda")
+        sur.predict_against(5, refs.data_ptr(), p2, ls, against.data_ptr())
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(against.cpu().numpy(), direct.cpu().numpy())
+
+
 def test_trained_surrogate_saves_exact_calls(gpu):
     import torch
     w = h = 512

@@ -93,6 +93,9 @@ def _declare(L):
     L.VshipExt_SurrogateInputs.argtypes = [HS, c.c_int, vpp, vpp, i64p, i64p, c.c_void_p, c.c_void_p]
     L.VshipExt_SurrogatePredictInputs.argtypes = [HS, c.c_int, c.c_void_p, c.c_void_p, c.c_void_p]
     L.VshipExt_SurrogatePredict.argtypes = [HS, c.c_int, vpp, vpp, i64p, i64p, c.c_void_p, c.c_void_p]
+    L.VshipExt_SurrogateReferenceSize.argtypes = [HS, i64p]
+    L.VshipExt_SurrogateReferences.argtypes = [HS, c.c_int, vpp, i64p, c.c_void_p, c.c_void_p]
+    L.VshipExt_SurrogatePredictAgainst.argtypes = [HS, c.c_int, c.c_void_p, vpp, i64p, c.c_void_p, c.c_void_p]
     L.VshipExt_SurrogateTrain.argtypes = [HS, c.c_int, c.c_void_p, c.c_void_p, c.c_int, c.c_int, c.c_float, c.c_uint,
                                           c.c_void_p]
     L.VshipExt_SurrogateGradients.argtypes = [HS, c.c_int, c.c_void_p, c.c_void_p, c.c_void_p,
@@ -447,6 +450,21 @@ class Surrogate:
         a2 = (ctypes.c_void_p * (3 * n))(*ptrs2)
         self._check(self.L.VshipExt_SurrogatePredict(self.h, n, a1, a2, abi.LineSizes(*line_sizes1),
                                                      abi.LineSizes(*line_sizes2), d_pred, stream or None))
+
+    def reference_floats(self):
+        n = ctypes.c_int64(0)
+        self._check(self.L.VshipExt_SurrogateReferenceSize(self.h, ctypes.byref(n)))
+        return n.value
+
+    def references(self, n, ptrs1, line_sizes1, d_refs, stream=0):
+        a1 = (ctypes.c_void_p * (3 * n))(*ptrs1)
+        self._check(self.L.VshipExt_SurrogateReferences(self.h, n, a1, abi.LineSizes(*line_sizes1), d_refs,
+                                                        stream or None))
+
+    def predict_against(self, n, d_refs, ptrs2, line_sizes2, d_pred, stream=0):
+        a2 = (ctypes.c_void_p * (3 * n))(*ptrs2)
+        self._check(self.L.VshipExt_SurrogatePredictAgainst(self.h, n, d_refs, a2, abi.LineSizes(*line_sizes2),
+                                                            d_pred, stream or None))
 
     def predict_inputs(self, n, d_inputs, d_pred, stream=0):
         self._check(self.L.VshipExt_SurrogatePredictInputs(self.h, n, d_inputs, d_pred, stream or None))

@@ -708,6 +708,36 @@ Vship_Exception VshipExt_SurrogatePredict(VshipExt_SurrogateHandler handler, int
     });
 }
 
+Vship_Exception VshipExt_SurrogateReferenceSize(VshipExt_SurrogateHandler handler, int64_t* floats) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateReferenceSize", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (!floats) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        *floats = s.engine->reference_floats();
+    });
+}
+
+Vship_Exception VshipExt_SurrogateReferences(VshipExt_SurrogateHandler handler, int n, const uint8_t* const* srcp1,
+                                             const int64_t lineSize[3], float* d_refs, void* stream) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateReferences", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 0) throw Error(Vship_BadPointer, __FILE__, __LINE__, "negative frame count");
+        if (n > 0 && (!srcp1 || !lineSize || !d_refs)) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->references(n, srcp1, lineSize, d_refs, (cudaStream_t)stream);
+    });
+}
+
+Vship_Exception VshipExt_SurrogatePredictAgainst(VshipExt_SurrogateHandler handler, int n, const float* d_refs,
+                                                 const uint8_t* const* srcp2, const int64_t lineSize2[3], float* d_pred,
+                                                 void* stream) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogatePredictAgainst", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        if (n < 0) throw Error(Vship_BadPointer, __FILE__, __LINE__, "negative pair count");
+        if (n > 0 && (!d_refs || !srcp2 || !lineSize2 || !d_pred))
+            throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->predict_against(n, d_refs, srcp2, lineSize2, d_pred, (cudaStream_t)stream);
+    });
+}
+
 Vship_Exception VshipExt_SurrogateTrain(VshipExt_SurrogateHandler handler, int n, const void* d_inputs,
                                         const float* d_targets, int epochs, int batch, float lr, unsigned seed,
                                         float* loss_history) {

@@ -73,6 +73,13 @@ struct SurrogateApi {
     // Inputs and predictions of n device-resident pairs (internal input buffer).
     virtual void predict(int n, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t ls1[3],
                          const int64_t ls2[3], float* d_pred, cudaStream_t stream) = 0;
+    // Levels 1/8 and 1/16 of n reference images (FP32, reference_floats() each), and
+    // predictions of n distorted images against such prepared references.
+    virtual int64_t reference_floats() const = 0;
+    virtual void references(int n, const uint8_t* const* d1, const int64_t ls1[3], float* d_refs,
+                            cudaStream_t stream) = 0;
+    virtual void predict_against(int n, const float* d_refs, const uint8_t* const* d2, const int64_t ls2[3],
+                                 float* d_pred, cudaStream_t stream) = 0;
     // Loss and gradients (FP32, num_params()) of the current weights on n samples.
     virtual double gradients(int n, const void* d_inputs, const float* d_targets, float* grads_host) = 0;
     virtual void train(int n, const void* d_inputs, const float* d_targets, int epochs, int batch, float lr,

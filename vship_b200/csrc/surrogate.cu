@@ -74,6 +74,7 @@ struct CoarseArgs {
     ColourParams cp[2];
     Pyramid pyr;                   // levels 3 and 4 stored, everything else -1
     float* out;                    // image i at out + i * pyr.image_floats
+    int clip;                      // -1: images alternate reference / distorted; else every image is this clip
     RawImage raw[2 * kMaxChunk];
 };
 
@@ -81,7 +82,7 @@ template <int kFast>
 __global__ void __launch_bounds__(256) sg_coarse_front_kernel(const __grid_constant__ CoarseArgs a) {
     __shared__ FrontSmem fs;
     extern __shared__ __align__(16) float stage[];
-    const int img = blockIdx.z, clip = img & 1;
+    const int img = blockIdx.z, clip = a.clip < 0 ? (img & 1) : a.clip;
     const LinearIn lin{};
     front_tile<false, kFast, true>(fs, stage, a.cp[clip], a.raw[img], lin, a.pyr,
                                    a.out + (int64_t)img * a.pyr.image_floats, blockIdx.x, blockIdx.y);
@@ -106,6 +107,49 @@ __global__ void sg_pack_kernel(const float* __restrict__ coarse, Pyramid pyr, Le
     for (int p = 0; p < 3; p++) {
         const int64_t o = pyr.off[L][p] + (int64_t)y * pyr.pitch[L] + x;
         const float va = A[o], vb = B[o];
+        out[p * plane + j] = __float2half_rn(va);
+        out[(3 + p) * plane + j] = __float2half_rn(vb - va);
+    }
+}
+
+// Reference levels of one image, dense FP32: [3][h3][w3] then [3][h4][w4].
+__global__ void sg_pack_reference_kernel(const float* __restrict__ coarse, Pyramid pyr, Level l3, Level l4,
+                                         int64_t ref_floats, float* __restrict__ refs) {
+    const int img = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n3 = l3.h * l3.w, n4 = l4.h * l4.w;
+    if (i >= n3 + n4) return;
+    const int L = i < n3 ? 3 : 4;
+    const Level& lv = i < n3 ? l3 : l4;
+    const int j = i < n3 ? i : i - n3;
+    const int y = j / lv.w, x = j - y * lv.w;
+    const float* A = coarse + (int64_t)img * pyr.image_floats;
+    float* out = refs + (int64_t)img * ref_floats + (i < n3 ? 0 : 3 * n3);
+    const int64_t plane = (int64_t)lv.h * lv.w;
+#pragma unroll
+    for (int p = 0; p < 3; p++) out[p * plane + j] = A[pyr.off[L][p] + (int64_t)y * pyr.pitch[L] + x];
+}
+
+// Network inputs of distorted images against prepared reference levels: the same values
+// sg_pack_kernel writes for the pair.
+__global__ void sg_pack_against_kernel(const float* __restrict__ coarse, Pyramid pyr, Level l3, Level l4,
+                                       const float* __restrict__ refs, int64_t ref_floats, int64_t block,
+                                       __half* __restrict__ inputs) {
+    const int pair = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n3 = l3.h * l3.w, n4 = l4.h * l4.w;
+    if (i >= n3 + n4) return;
+    const int L = i < n3 ? 3 : 4;
+    const Level& lv = i < n3 ? l3 : l4;
+    const int j = i < n3 ? i : i - n3;
+    const int y = j / lv.w, x = j - y * lv.w;
+    const float* A = refs + (int64_t)pair * ref_floats + (i < n3 ? 0 : 3 * n3);
+    const float* B = coarse + (int64_t)pair * pyr.image_floats;
+    __half* out = inputs + (int64_t)pair * block + lv.off;
+    const int64_t plane = (int64_t)lv.h * lv.w;
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        const float va = A[p * plane + j], vb = B[pyr.off[L][p] + (int64_t)y * pyr.pitch[L] + x];
         out[p * plane + j] = __float2half_rn(va);
         out[(3 + p) * plane + j] = __float2half_rn(vb - va);
     }
@@ -477,51 +521,108 @@ public:
     int64_t input_elems() const override { return block_; }
     int num_params() const override { return kParams; }
 
-    void inputs(int n, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t ls1[3], const int64_t ls2[3],
-                void* d_inputs, cudaStream_t stream) override {
-        ColourParams cp[2] = {cp_[0], cp_[1]};
+    // Colour parameters of both clips for these strides (validated; a null stride array
+    // skips its clip).
+    void validate(const int64_t ls1[3], const int64_t ls2[3], ColourParams cp[2]) const {
+        cp[0] = cp_[0];
+        cp[1] = cp_[1];
         for (int c = 0; c < 2; c++) {
             const int64_t* ls = c ? ls2 : ls1;
+            if (!ls) continue;
             for (int p = 0; p < 3; p++) {
                 if (ls[p] < geo_[c].pw[p] * geo_[c].bytes) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
                 if (ls[p] % geo_[c].bytes) cp[c].misaligned = 1;
             }
         }
+    }
+
+    // Levels 3 and 4 of `chunk` images into coarse_: pairs (clip -1: d1 and d2 interleaved),
+    // or the images of one clip (0: d1, 1: d2).
+    void coarse_front(int chunk, int clip, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t* ls1,
+                      const int64_t* ls2, const ColourParams cp[2], cudaStream_t stream) {
+        CoarseArgs& a = coarse_args_;
+        a.cp[0] = cp[0];
+        a.cp[1] = cp[1];
+        a.pyr = pyr_;
+        a.out = coarse_;
+        a.clip = clip;
+        const int per = clip < 0 ? 2 : 1;
+        for (int i = 0; i < chunk; i++)
+            for (int k = 0; k < per; k++) {
+                const int c = clip < 0 ? k : clip;
+                const uint8_t* const* src = c ? d2 : d1;
+                RawImage& r = a.raw[per * i + k];
+                for (int p = 0; p < 3; p++) {
+                    if (!src[3 * i + p]) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
+                    r.p[p] = src[3 * i + p];
+                    r.stride[p] = (c ? ls2 : ls1)[p];
+                }
+                if (misaligned_view(r, geo_[c])) a.cp[c].misaligned = 1;
+            }
+        const int f0 = fast_path_of(a.cp[0]), f1 = fast_path_of(a.cp[1]);
+        const int fast = clip == 0 ? f0 : clip == 1 ? f1 : (f0 == f1 ? f0 : kFastGeneric);
+        const int smem = (int)sizeof(float) * std::max(chroma_stage_floats(a.cp[0].subw, a.cp[0].subh),
+                                                       chroma_stage_floats(a.cp[1].subw, a.cp[1].subh));
+        auto kern = fast == kFastYuv420Bt709 ? sg_coarse_front_kernel<kFastYuv420Bt709>
+                  : fast == kFastRgb8Srgb ? sg_coarse_front_kernel<kFastRgb8Srgb>
+                                          : sg_coarse_front_kernel<kFastGeneric>;
+        if (smem > 32 * 1024) CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        const dim3 grid((unsigned)ceil_div(pyr_.w[1], 32), (unsigned)ceil_div(pyr_.h[1], 32), (unsigned)(per * chunk));
+        const int t = timer_.begin(0, "surrogate_coarse_front", stream);
+        kern<<<grid, 256, smem, stream>>>(a);
+        CUDA_CHECK(cudaGetLastError());
+        timer_.end(t, stream);
+    }
+
+    void inputs(int n, const uint8_t* const* d1, const uint8_t* const* d2, const int64_t ls1[3], const int64_t ls2[3],
+                void* d_inputs, cudaStream_t stream) override {
+        ColourParams cp[2];
+        validate(ls1, ls2, cp);
         __half* out = static_cast<__half*>(d_inputs);
         for (int done = 0; done < n; done += kMaxChunk) {
             const int chunk = std::min(kMaxChunk, n - done);
-            CoarseArgs& a = coarse_args_;
-            a.cp[0] = cp[0];
-            a.cp[1] = cp[1];
-            a.pyr = pyr_;
-            a.out = coarse_;
-            for (int i = 0; i < chunk; i++)
-                for (int c = 0; c < 2; c++) {
-                    const uint8_t* const* src = c ? d2 : d1;
-                    for (int p = 0; p < 3; p++) {
-                        if (!src[3 * (done + i) + p]) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
-                        a.raw[2 * i + c].p[p] = src[3 * (done + i) + p];
-                        a.raw[2 * i + c].stride[p] = (c ? ls2 : ls1)[p];
-                    }
-                    if (misaligned_view(a.raw[2 * i + c], geo_[c])) a.cp[c].misaligned = 1;
-                }
-            const int f0 = fast_path_of(a.cp[0]), f1 = fast_path_of(a.cp[1]);
-            const int fast = f0 == f1 ? f0 : kFastGeneric;
-            const int smem = (int)sizeof(float) * std::max(chroma_stage_floats(a.cp[0].subw, a.cp[0].subh),
-                                                           chroma_stage_floats(a.cp[1].subw, a.cp[1].subh));
-            auto kern = fast == kFastYuv420Bt709 ? sg_coarse_front_kernel<kFastYuv420Bt709>
-                      : fast == kFastRgb8Srgb ? sg_coarse_front_kernel<kFastRgb8Srgb>
-                                              : sg_coarse_front_kernel<kFastGeneric>;
-            if (smem > 32 * 1024) CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            const dim3 grid((unsigned)ceil_div(pyr_.w[1], 32), (unsigned)ceil_div(pyr_.h[1], 32), (unsigned)(2 * chunk));
-            const int t = timer_.begin(0, "surrogate_coarse_front", stream);
-            kern<<<grid, 256, smem, stream>>>(a);
-            CUDA_CHECK(cudaGetLastError());
-            timer_.end(t, stream);
+            coarse_front(chunk, -1, d1 + 3 * done, d2 + 3 * done, ls1, ls2, cp, stream);
             const int npx = l3_.h * l3_.w + l4_.h * l4_.w;
             sg_pack_kernel<<<dim3((unsigned)ceil_div(npx, 256), (unsigned)chunk), 256, 0, stream>>>(
                 coarse_, pyr_, l3_, l4_, block_, out + (int64_t)done * block_);
             CUDA_CHECK(cudaGetLastError());
+        }
+    }
+
+    int64_t reference_floats() const override { return 3 * ((int64_t)l3_.h * l3_.w + (int64_t)l4_.h * l4_.w); }
+
+    void references(int n, const uint8_t* const* d1, const int64_t ls1[3], float* d_refs, cudaStream_t stream) override {
+        ColourParams cp[2];
+        validate(ls1, nullptr, cp);
+        for (int done = 0; done < n; done += kMaxChunk) {
+            const int chunk = std::min(kMaxChunk, n - done);
+            coarse_front(chunk, 0, d1 + 3 * done, nullptr, ls1, nullptr, cp, stream);
+            const int npx = l3_.h * l3_.w + l4_.h * l4_.w;
+            sg_pack_reference_kernel<<<dim3((unsigned)ceil_div(npx, 256), (unsigned)chunk), 256, 0, stream>>>(
+                coarse_, pyr_, l3_, l4_, reference_floats(), d_refs + (int64_t)done * reference_floats());
+            CUDA_CHECK(cudaGetLastError());
+        }
+    }
+
+    void predict_against(int n, const float* d_refs, const uint8_t* const* d2, const int64_t ls2[3], float* d_pred,
+                         cudaStream_t stream) override {
+        ColourParams cp[2];
+        validate(nullptr, ls2, cp);
+        constexpr int kChunk = 256;
+        if (!pred_inputs_) pred_inputs_ = device_alloc<__half>((size_t)kChunk * block_, "surrogate prediction inputs");
+        for (int base = 0; base < n; base += kChunk) {
+            const int count = std::min(kChunk, n - base);
+            for (int done = 0; done < count; done += kMaxChunk) {
+                const int chunk = std::min(kMaxChunk, count - done);
+                const int first = base + done;
+                coarse_front(chunk, 1, nullptr, d2 + 3 * first, nullptr, ls2, cp, stream);
+                const int npx = l3_.h * l3_.w + l4_.h * l4_.w;
+                sg_pack_against_kernel<<<dim3((unsigned)ceil_div(npx, 256), (unsigned)chunk), 256, 0, stream>>>(
+                    coarse_, pyr_, l3_, l4_, d_refs + (int64_t)first * reference_floats(), reference_floats(), block_,
+                    pred_inputs_ + (int64_t)done * block_);
+                CUDA_CHECK(cudaGetLastError());
+            }
+            predict_inputs(count, pred_inputs_, d_pred + base, stream);
         }
     }
 

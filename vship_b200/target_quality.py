@@ -3,10 +3,11 @@
 A target-quality encoder looks, per frame, for the coarsest quantisation whose SSIMULACRA2
 stays at or above a target (80 here).  Bisection over the quantisation step needs one score
 per probe; most probes land far from the target, where only the side of the threshold
-matters.  `search` consults the surrogate (VshipExt_SurrogatePredict) for every probe and
-calls the exact metric only when the prediction is within `margin` of the target; the exact
-metric also judges the surrogate's error on those probes.  `search(..., surrogate=None)` is
-the method without it (every probe exact).
+matters.  `search` consults the surrogate for every probe (the reference's coarse levels
+prepared once per frame, VshipExt_SurrogateReferences, then VshipExt_SurrogatePredictAgainst
+per probe) and calls the exact metric only when the prediction is within `margin` of the
+target; the exact metric also judges the surrogate's error on those probes.
+`search(..., surrogate=None)` is the method without it (every probe exact).
 
 Frames come from `GpuFrames`, the generator of vship_b200.synth moved to the GPU with torch
 (seeded sums of random sinusoids plus noise; the distortion is 8x8 block-DCT quantisation
@@ -150,6 +151,14 @@ def search(frames_yuv_fn, distort_fn, nframes, exact, surrogate=None, target=80.
     exact_calls, probes, errors = 0, 0, []
     pred = torch.empty(batch, dtype=torch.float32, device="cuda")
     ex = torch.empty(batch, dtype=torch.float64, device="cuda")
+    refs = None
+    if surrogate is not None:
+        # Every probe of a frame shares its reference: its coarse levels are computed once.
+        refs = torch.empty((nframes, surrogate.reference_floats()), dtype=torch.float32, device="cuda")
+        for i0 in range(0, nframes, batch):
+            i1 = min(nframes, i0 + batch)
+            p1, ls = planes_of(frames_yuv_fn(i0, i1))
+            surrogate.references(i1 - i0, p1, ls, refs[i0].data_ptr())
     for _ in range(iters):
         mid = 0.5 * (lo_s + hi_s)
         for i0 in range(0, nframes, batch):
@@ -161,7 +170,7 @@ def search(frames_yuv_fn, distort_fn, nframes, exact, surrogate=None, target=80.
             p2, _ = planes_of(b)
             probes += k
             if surrogate is not None:
-                surrogate.predict(k, p1, p2, ls, ls, pred.data_ptr())
+                surrogate.predict_against(k, refs[i0].data_ptr(), p2, ls, pred.data_ptr())
                 score = pred[:k].double().cpu().numpy()
                 near = np.abs(score - target) <= margin
             else:
