@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kMapThreads) ssimu2_maps_kernel(const __grid_c
     load_halo<kTile, false>(cur, regs);
 
     while (true) {
-        stage_halo<kTile>(sm, regs);
+        stage_halo<kTile>(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
         const int X0 = cur.X0, Y0 = cur.Y0, w = cur.w, h = cur.h;
         const int next = tile + gridDim.x;
         if (next < total_tiles) {

@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kMapThreads, TH == 64 ? 3 : 4) ssimu2_batch_ma
             gate.wait(v, pair);
             load_halo<TH, true>(cur, regs);
         }
-        stage_halo<TH>(sm, regs);
+        stage_halo<TH>(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
         const TileRef t = cur;
         const unsigned tpartial = partial;
         const int next = m + stride;

@@ -249,6 +249,8 @@ struct MapTile {
         float2 hab[kRows][kTile + 1];
         float2 hpq[kRows][kTile + 1];
         double red[kMapThreads / 32][6];
+        float invx[kTile];    // 1 / in-plane tap weight of each output column of the tile
+        float invy[TH];       // ... and of each output row
         float shift;
     };
     struct Regs {
@@ -281,11 +283,19 @@ __device__ __forceinline__ void load_halo(const TileRef& t, typename MapTile<TH>
     }
 }
 
-// Moves a loaded halo into shared memory, shifted by the tile constant k; ends with a
-// barrier, after which the registers are free for the next tile's loads.
+// Moves a loaded halo into shared memory, shifted by the tile constant k, and tabulates the
+// renormalisation of the tile's output columns and rows (tile origin X0, Y0 in a w x h
+// plane; positions past the plane, whose outputs are never used, take the last in-plane
+// one).  Ends with a barrier, after which the registers are free for the next tile's loads.
 template <int TH>
-__device__ __forceinline__ void stage_halo(typename MapTile<TH>::Smem& sm, const typename MapTile<TH>::Regs& r) {
+__device__ __forceinline__ void stage_halo(typename MapTile<TH>::Smem& sm, const typename MapTile<TH>::Regs& r,
+                                           int X0, int Y0, int w, int h) {
     const int tid = threadIdx.x;
+    static_assert(kTile + TH <= kMapThreads, "one renormalisation entry per thread");
+    if (tid < kTile)
+        sm.invx[tid] = 1.0f / blur_norm(min(X0 + tid, w - 1), w);
+    else if (tid < kTile + TH)
+        sm.invy[tid - kTile] = 1.0f / blur_norm(min(Y0 + tid - kTile, h - 1), h);
     // Shift constant k: the mean of both images at the tile's first output pixel (halo
     // element (8, 8), held by thread 8 as its 4th element; always inside the image).
     // The renormalised blur maps constants to themselves, so moments of a-k, b-k give the
@@ -344,7 +354,7 @@ __device__ __forceinline__ void blur_score_tile(typename MapTile<TH>::Smem& sm, 
         }
 #pragma unroll
         for (int o = 0; o < 4; o++) {
-            const float inv = 1.0f / blur_norm(X0 + c0 + o, w);
+            const float inv = sm.invx[c0 + o];
             sm.hab[r][c0 + o] = f2(acc_ab[o].x * inv, acc_ab[o].y * inv);
             sm.hpq[r][c0 + o] = f2(acc_pq[o].x * inv, acc_pq[o].y * inv);
         }
@@ -386,7 +396,7 @@ __device__ __forceinline__ void blur_score_tile(typename MapTile<TH>::Smem& sm, 
         for (int o = 0; o < RPT; o++) {
             const int gy = Y0 + r0 + o;
             if (gx >= w || gy >= h) continue;
-            const float inv = 1.0f / blur_norm(gy, h);
+            const float inv = sm.invy[r0 + o];
             // Shifted means m1 = mu1 - k, m2 = mu2 - k, s12 = blur((a-k)(b-k)), D = blur((a-b)^2).
             const float m1 = mab[o].x * inv, m2 = mab[o].y * inv, s12 = mpq[o].x * inv, D = mpq[o].y * inv;
             // SSIM map of the reference (src/ssimu2/score.hpp:266-274),
@@ -398,12 +408,13 @@ __device__ __forceinline__ void blur_score_tile(typename MapTile<TH>::Smem& sm, 
             const float md2 = md * md;
             const float N = fmaf(2.0f, s12 - m1 * m2, 0.0009f);
             const float V = D - md2;
-            const float ssim = fmaxf(fmaf(md2, N, V) / (V + N), 0.0f);
+            // V + N = s1^2 + s2^2 + C >= C > 0: the fast division (2 ulp) is safe here.
+            const float ssim = fmaxf(__fdividef(fmaf(md2, N, V), V + N), 0.0f);
             // Artifact and detail-loss maps (score.hpp:276-281): (|b-mu2|+1)/(|a-mu1|+1) - 1,
             // evaluated as (|b-mu2| - |a-mu1|) / (|a-mu1| + 1) to avoid cancelling against 1.
             const float2 cv = sm.sab[r0 + o + kHalo][c + kHalo];
             const float ea = fabsf(cv.x - m1), eb = fabsf(cv.y - m2);
-            const float v1 = (eb - ea) / (ea + 1.0f);
+            const float v1 = __fdividef(eb - ea, ea + 1.0f);
             const float art = fmaxf(v1, 0.0f), det = fmaxf(-v1, 0.0f);
             const float s2 = ssim * ssim, a2 = art * art, d2 = det * det;
             sum[0] += ssim; sum[1] += art; sum[2] += det;
