@@ -277,6 +277,8 @@ __device__ __forceinline__ float3 primaries_to_709(float3 v, int prim) {
 // starts and fractions of the tile's 64 columns and rows come from small phase tables.
 // ---------------------------------------------------------------------------------------
 constexpr int kStageTile = 64;
+// Front paths (see fast_path_of): the generic runtime-dispatched one and two compile-time ones.
+constexpr int kFastGeneric = 0, kFastYuv420Bt709 = 1, kFastRgb8Srgb = 2;
 constexpr int kStageMaxSpan = kStageTile + 4;  // staged rows/columns: interval range + 3 taps
 
 struct ChromaStage {
@@ -311,6 +313,10 @@ __device__ __forceinline__ void phase32(int X, int sub, int centered, int& i, fl
     }
 }
 
+// kFast names the front path: for 16-bit 4:2:0 samples (kFastYuv420Bt709) each thread owns
+// one staged column and issues all its row loads before using any, so a tile waits for
+// memory about once instead of once per row.  Both paths stage the same values.
+template <int kFast = kFastGeneric>
 __device__ __forceinline__ void chroma_stage(const RawImage& im, const ColourParams& cp, int X0, int Y0, float* smem,
                                              ChromaStage& st) {
     const int W = (int)cp.W, H = (int)cp.H, cw = (int)cp.cw, ch = (int)cp.ch;
@@ -356,12 +362,44 @@ __device__ __forceinline__ void chroma_stage(const RawImage& im, const ColourPar
         st.vt[tid - kStageTile] = f;
     }
     const bool chroma = cp.yuv_chroma != 0;
-    for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
-        const int p = r >= st.cy_n, rr = r - p * st.cy_n;
-        const int gy = min(max(st.cy_lo + rr, 0), ch - 1);
-        for (int c = lane; c < st.cx_n; c += 32) {
+    if constexpr (kFast == kFastYuv420Bt709) {  // aligned 16-bit samples, cx_n <= 36 columns
+        constexpr int kBatch = 19;
+        const int c = tid & 63, ng = blockDim.x >> 6, rows = 2 * st.cy_n;
+        if (c < st.cx_n) {
             const int gx = min(max(st.cx_lo + c, 0), cw - 1);
-            st.S[r * kStageMaxSpan + c] = load_norm(im.p[1 + p], im.stride[1 + p], gx, gy, cp, chroma);
+            for (int r0 = tid >> 6; r0 < rows; r0 += ng * kBatch) {
+                unsigned short u[kBatch];
+#pragma unroll
+                for (int k = 0; k < kBatch; k++) {
+                    const int r = r0 + k * ng;
+                    u[k] = 0;
+                    if (r < rows) {
+                        const int p = r >= st.cy_n, rr = r - p * st.cy_n;
+                        const int gy = min(max(st.cy_lo + rr, 0), ch - 1);
+                        u[k] = __ldg(reinterpret_cast<const unsigned short*>(im.p[1 + p] + (int64_t)gy * im.stride[1 + p]) + gx);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kBatch; k++) {
+                    const int r = r0 + k * ng;
+                    if (r < rows) {
+                        float v = (float)(u[k] & cp.mask);
+                        // FullRange of a chroma sample, as load_norm computes it.
+                        if (cp.full_range) v = v * cp.full_scale - 0.5f;
+                        else v = (v * cp.lim_scale - 128.f) * (1.0f / 224.f);
+                        st.S[r * kStageMaxSpan + c] = v;
+                    }
+                }
+            }
+        }
+    } else {
+        for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
+            const int p = r >= st.cy_n, rr = r - p * st.cy_n;
+            const int gy = min(max(st.cy_lo + rr, 0), ch - 1);
+            for (int c = lane; c < st.cx_n; c += 32) {
+                const int gx = min(max(st.cx_lo + c, 0), cw - 1);
+                st.S[r * kStageMaxSpan + c] = load_norm(im.p[1 + p], im.stride[1 + p], gx, gy, cp, chroma);
+            }
         }
     }
     __syncthreads();
@@ -442,8 +480,8 @@ __device__ __forceinline__ float3 ingest_pixel(const RawImage& im, int64_t X, in
 // time.
 //   kFastYuv420Bt709: 16-bit containers, 4:2:0, Left siting, BT.709 matrix, transfer, primaries
 //   kFastRgb8Srgb:    8-bit R'G'B' 4:4:4, sRGB transfer, BT.709 primaries
+// (kFastGeneric, kFastYuv420Bt709, kFastRgb8Srgb are declared before chroma_stage.)
 // ---------------------------------------------------------------------------------------
-constexpr int kFastGeneric = 0, kFastYuv420Bt709 = 1, kFastRgb8Srgb = 2;
 
 __host__ __device__ inline int fast_path_of(const ColourParams& cp) {
     const bool u16 = cp.sample != Vship_SampleUINT8 && cp.sample != Vship_SampleFLOAT && cp.sample != Vship_SampleHALF;

@@ -142,7 +142,7 @@ __device__ __forceinline__ void front_tile(FrontSmem& fs, float* stage_mem, cons
     const int X0t = tx * kStageTile, Y0t = ty * kStageTile;
     ChromaStage st{};
     if (!FromLinear && kFast != kFastRgb8Srgb && (cp.subw || cp.subh))
-        chroma_stage(im, cp, X0t, Y0t, stage_mem, st);
+        chroma_stage<kFast>(im, cp, X0t, Y0t, stage_mem, st);
 
     auto pixel = [&](int X, int Y) -> float3 {
         if (FromLinear) {
