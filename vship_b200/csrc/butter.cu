@@ -118,11 +118,30 @@ static void upload_constants() {
 // Tiled separable blur helper
 // ------------------------------------------------------------------------------------------
 
-template <int R>
+// One or two planes per blur: two planes travel as float2 through shared memory so that one
+// packed FP32x2 FMA (sm_100) serves both, halving the tap arithmetic.
+template <int NP> struct BlurVec;
+template <> struct BlurVec<1> {
+    using T = float;
+    __device__ static float zero() { return 0.f; }
+    __device__ static float fma(float g, float x, float acc) { return fmaf(x, g, acc); }
+    __device__ static float scale(float x, float s) { return x * s; }
+};
+template <> struct BlurVec<2> {
+    using T = float2;
+    __device__ static float2 zero() { return make_float2(0.f, 0.f); }
+    __device__ static float2 fma(float g, float2 x, float2 acc) { return __ffma2_rn(x, make_float2(g, g), acc); }
+    __device__ static float2 scale(float2 x, float s) { return make_float2(x.x * s, x.y * s); }
+};
+
+template <int R, int NP>
 struct BlurSmem {
+    using V = typename BlurVec<NP>::T;
     static constexpr int IN = kTile + 2 * R;
-    float in[IN][IN + 1];
-    float h[IN][kTile + 1];
+    V in[IN][IN + 1];
+    V h[IN][kTile + 1];
+    float invx[kTile];   // 1 / in-image tap weight of each output column
+    float invy[kTile];   // ... and row
 };
 
 __device__ __forceinline__ float tap_sum(int k, int R, int pos, int n) {
@@ -131,52 +150,82 @@ __device__ __forceinline__ float tap_sum(int k, int R, int pos, int n) {
     return c_prefix[k][end] - c_prefix[k][beg];
 }
 
-// Blurs one plane over the CTA's 32x32 tile (origin X0, Y0).  `src(x, y)` returns the input
-// at an in-image position.  Thread t gets column t&31, rows 4*(t>>5) .. +3 in out[0..3].
-template <int R, int K, typename Src>
-__device__ __forceinline__ void blur_tile(BlurSmem<R>& sm, Src src, int X0, int Y0, int w, int h, float out[4]) {
-    constexpr int IN = BlurSmem<R>::IN;
+// Blurs NP planes over the CTA's 32x32 tile (origin X0, Y0): `src(x, y)` returns the input
+// (a float, or a float2 of the two planes) at an in-image position.  Thread t gets column
+// t&31, rows 4*(t>>5) .. +3 in out[0..3].  The per-position renormalisation (divide by the
+// in-image tap weight, src/butter/gaussianblur.hpp) is applied as a tabulated reciprocal.
+template <int R, int K, int NP, typename Src>
+__device__ __forceinline__ void blur_tile(BlurSmem<R, NP>& sm, Src src, int X0, int Y0, int w, int h,
+                                          typename BlurVec<NP>::T out[4]) {
+    using B = BlurVec<NP>;
+    using V = typename B::T;
+    constexpr int IN = BlurSmem<R, NP>::IN;
     constexpr int NT = 2 * R + 1;
     const int tid = threadIdx.x;
     for (int i = tid; i < IN * IN; i += 256) {
         const int r = i / IN, c = i % IN;
         const int gx = X0 - R + c, gy = Y0 - R + r;
-        sm.in[r][c] = (gx >= 0 && gx < w && gy >= 0 && gy < h) ? src(gx, gy) : 0.f;
+        sm.in[r][c] = (gx >= 0 && gx < w && gy >= 0 && gy < h) ? src(gx, gy) : B::zero();
     }
+    if (tid < kTile)
+        sm.invx[tid] = 1.0f / tap_sum(K, R, min(X0 + tid, w - 1), w);
+    else if (tid < 2 * kTile)
+        sm.invy[tid - kTile] = 1.0f / tap_sum(K, R, min(Y0 + tid - kTile, h - 1), h);
     __syncthreads();
     for (int u = tid; u < IN * (kTile / 2); u += 256) {
         const int r = u >> 4, c0 = (u & 15) * 2;
-        float a0 = 0.f, a1 = 0.f;
-        float prev = sm.in[r][c0];
+        V a0 = B::zero(), a1 = B::zero();
+        V prev = sm.in[r][c0];
 #pragma unroll
         for (int j = 0; j < NT; j++) {
             const float g = c_taps[K][j];
-            const float nxt = sm.in[r][c0 + j + 1];
-            a0 = fmaf(prev, g, a0);
-            a1 = fmaf(nxt, g, a1);
+            const V nxt = sm.in[r][c0 + j + 1];
+            a0 = B::fma(g, prev, a0);
+            a1 = B::fma(g, nxt, a1);
             prev = nxt;
         }
-        sm.h[r][c0] = a0 / tap_sum(K, R, X0 + c0, w);
-        sm.h[r][c0 + 1] = a1 / tap_sum(K, R, X0 + c0 + 1, w);
+        sm.h[r][c0] = B::scale(a0, sm.invx[c0]);
+        sm.h[r][c0 + 1] = B::scale(a1, sm.invx[c0 + 1]);
     }
     __syncthreads();
     const int c = tid & 31, r0 = (tid >> 5) * 4;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    V acc[4] = {B::zero(), B::zero(), B::zero(), B::zero()};
 #pragma unroll
     for (int j = 0; j < NT + 3; j++) {
-        const float v = sm.h[r0 + j][c];
+        const V v = sm.h[r0 + j][c];
 #pragma unroll
         for (int o = 0; o < 4; o++) {
             const int t = j - o;
-            if (t >= 0 && t < NT) acc[o] = fmaf(v, c_taps[K][t], acc[o]);
+            if (t >= 0 && t < NT) acc[o] = B::fma(c_taps[K][t], v, acc[o]);
         }
     }
 #pragma unroll
     for (int o = 0; o < 4; o++) {
         const int gy = Y0 + r0 + o;
-        out[o] = gy < h ? acc[o] / tap_sum(K, R, gy, h) : 0.f;
+        out[o] = gy < h ? B::scale(acc[o], sm.invy[r0 + o]) : B::zero();
     }
     __syncthreads();
+}
+
+// Two-plane and one-plane blurs of the same radius sharing one shared-memory block.
+template <int R>
+union BlurSmemPair {
+    BlurSmem<R, 2> two;
+    BlurSmem<R, 1> one;
+};
+
+// Blurs three planes (two packed, one alone) with the same kernel; bl[c][o] as blur_tile.
+template <int R, int K, typename Src>
+__device__ __forceinline__ void blur_three(BlurSmemPair<R>& sm, Src src, int X0, int Y0, int w, int h,
+                                           float bl[3][4]) {
+    float2 b01[4];
+    blur_tile<R, K, 2>(sm.two, [&](int x, int y) { return make_float2(src(0, x, y), src(1, x, y)); }, X0, Y0, w, h, b01);
+    blur_tile<R, K, 1>(sm.one, [&](int x, int y) { return src(2, x, y); }, X0, Y0, w, h, bl[2]);
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+        bl[0][o] = b01[o].x;
+        bl[1][o] = b01[o].y;
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -217,15 +266,11 @@ __device__ __forceinline__ float butter_gamma(float v) {  // colors.hpp:3-5
 
 // opsinDynamicsImage (colors.hpp:57-91).
 __global__ void __launch_bounds__(256) opsin_kernel(Planes P) {
-    __shared__ BlurSmem<8> sm;
+    __shared__ BlurSmemPair<8> sm;
     const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kTile;
     float bl[3][4];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const float* src = P.lin[c];
-        const int w = P.w;
-        blur_tile<8, 0>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl[c]);
-    }
+    const int w = P.w;
+    blur_three<8, 0>(sm, [&](int c, int x, int y) { return P.lin[c][(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl);
     const int c = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 4;
     const int x = X0 + c;
     if (x >= P.w) return;
@@ -255,15 +300,18 @@ __global__ void __launch_bounds__(256) opsin_kernel(Planes P) {
 }
 
 // Low-frequency split (separatefrequencies.hpp:160-176, XybLowFreqToVals :3-12).
+// Three scalar passes: a packed two-plane tile of radius 21 needs 64 KB of shared memory and
+// the occupancy it costs outweighs the halved tap arithmetic (measured 1.06 against 0.99 ms
+// per 4K pair).
 __global__ void __launch_bounds__(256) lf_kernel(Planes P) {
-    __shared__ BlurSmem<21> sm;
+    __shared__ BlurSmem<21, 1> sm;
     const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kTile;
     float bl[3][4];
+    const int w = P.w;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         const float* src = P.xyb[c];
-        const int w = P.w;
-        blur_tile<21, 4>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl[c]);
+        blur_tile<21, 4, 1>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl[c]);
     }
     const int c = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 4;
     const int x = X0 + c;
@@ -297,15 +345,11 @@ __device__ __forceinline__ float maximum_clamp(float v, float maxval) {
 
 // Medium-frequency split and X-by-Y suppression (separatefrequencies.hpp:161-187).
 __global__ void __launch_bounds__(256) mf_kernel(Planes P) {
-    __shared__ BlurSmem<9> sm;
+    __shared__ BlurSmemPair<9> sm;
     const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kTile;
     float bl[3][4];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const float* src = P.d[c];
-        const int w = P.w;
-        blur_tile<9, 3>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl[c]);
-    }
+    const int w = P.w;
+    blur_three<9, 3>(sm, [&](int c, int x, int y) { return P.d[c][(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl);
     const int c = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 4;
     const int x = X0 + c;
     if (x >= P.w) return;
@@ -329,14 +373,21 @@ __global__ void __launch_bounds__(256) mf_kernel(Planes P) {
 // High / ultra-high split (separatefrequencies.hpp:189-200, :117-133) and the psycho-mask
 // precompute of this image (maskPsycho.hpp:4-40, 120-128).
 __global__ void __launch_bounds__(256) hf_kernel(Planes P) {
-    __shared__ BlurSmem<8> sm;
+    __shared__ BlurSmem<8, 2> sm;
     const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kTile;
     float bl[2][4];
+    const int w = P.w;
+    {
+        float2 b01[4];
+        blur_tile<8, 1, 2>(sm, [&](int x, int y) {
+            const int64_t i = (int64_t)y * w + x;
+            return make_float2(P.hfpre[0][i], P.hfpre[1][i]);
+        }, X0, Y0, P.w, P.h, b01);
 #pragma unroll
-    for (int c = 0; c < 2; c++) {
-        const float* src = P.hfpre[c];
-        const int w = P.w;
-        blur_tile<8, 1>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl[c]);
+        for (int o = 0; o < 4; o++) {
+            bl[0][o] = b01[o].x;
+            bl[1][o] = b01[o].y;
+        }
     }
     const int c = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 4;
     const int x = X0 + c;
@@ -370,12 +421,12 @@ __global__ void __launch_bounds__(256) hf_kernel(Planes P) {
 
 // Blur of the mask precompute (maskPsycho.hpp:129-132).
 __global__ void __launch_bounds__(256) mask_kernel(Planes P) {
-    __shared__ BlurSmem<8> sm;
+    __shared__ BlurSmem<8, 1> sm;
     const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kTile;
     float bl[4];
     const float* src = P.p;
     const int w = P.w;
-    blur_tile<8, 2>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl);
+    blur_tile<8, 2, 1>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl);
     const int c = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 4;
     const int x = X0 + c;
     if (x >= P.w) return;

@@ -188,7 +188,15 @@ __device__ __forceinline__ float3 linear_light(float3 v, int matrix) {
 // |a|^g with the sign of a, as exp2(g * log2|a|) on the special-function unit.  The relative
 // error is ~3e-7 (log2 to 2^-21, exp2 to 2 ulp, times g), far below the metric's
 // resolution; pow's exact corner cases are not needed for finite pixel values.
-__device__ __forceinline__ float fast_pow(float x, float g) { return x > 0.f ? exp2f(g * __log2f(x)) : 0.f; }
+// 2^x on the special-function unit (PTX ex2.approx: relative error below 2^-22; results
+// below 2^-126 flush to zero).
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float fast_pow(float x, float g) { return x > 0.f ? ex2_approx(g * __log2f(x)) : 0.f; }
 __device__ __forceinline__ float signed_powf(float a, float g) { return a < 0 ? -fast_pow(-a, g) : fast_pow(a, g); }
 
 __device__ __forceinline__ float trc_one(float a, int trc) {

@@ -43,7 +43,7 @@ static __constant__ double c_weights[108] = {VSHIP_SSIMU2_WEIGHT_LIST};
 // Newton step y <- (2y + x / y^2) / 3, which leaves ~1 ulp of error.
 __device__ __forceinline__ float fast_cbrt(float x) {
     if (!(x > 0.f)) return 0.f;
-    float y = exp2f(__log2f(x) * (1.0f / 3.0f));
+    float y = ex2_approx(__log2f(x) * (1.0f / 3.0f));
     y = (2.0f * y + __fdividef(x, y * y)) * (1.0f / 3.0f);
     return y;
 }
