@@ -453,6 +453,102 @@ def run_butteraugli(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+CMETRIC = "1080p CVVDP frames/s"
+CWORKLOAD = "cvvdp_1080p_yuv420p10_bt709_24fps_standard_fhd"
+CFRAMES = 24  # frames per step and sequence: one second of 24 fps video
+
+
+def run_cvvdp(args, rank, local, reference=False):
+    """CVVDP over 1080p 10-bit 4:2:0 BT.709 sequences at 24 fps on the standard_fhd display,
+    end to end through Vship_ComputeCVVDP with pinned host frames (the reference has no
+    device-pointer entry); T concurrent sequences, each on its own handler and host thread,
+    best of the swept T.  Both arms run the same frames; one step is CFRAMES frames of every
+    sequence."""
+    import threading
+    import torch
+    from vship_b200 import abi, api, synth
+    torch.cuda.set_device(local)
+    lib = None
+    if reference:
+        ref_path = os.path.join(ROOT, "oracle", "_ref", "libvship_ref.so")
+        if not os.path.exists(ref_path):
+            print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/build_ref.sh)"}))
+            return
+        lib = api.load_library(ref_path)
+    t = time.time()
+    pairs = synth.make_pairs(8, W, H, fmt="yuv420p10", seed=91 + rank, unique=8, steps=(4.0, 48.0))
+    log("generated %d frame pairs in %.1fs" % (len(pairs), time.time() - t))
+    cs = abi.yuv420_10bit_bt709(W, H)
+    pinned, host_pairs = pinned_frames(pairs, api, lib=lib)
+    ls = pairs[0][2]
+    sweep = {}
+    best = None
+    for nthreads in args.cvvdp_threads:
+        handlers = [api.CVVDP(cs, fps=24.0, model="standard_fhd", gpu_id=local, lib=lib) for _ in range(nthreads)]
+        scores = [[] for _ in range(nthreads)]
+
+        def worker(i, frames):
+            h = handlers[i]
+            for f in range(frames):
+                a, b = host_pairs[(f + i) % len(host_pairs)]
+                scores[i].append(h.compute(a, b, ls, ls))
+
+        def run(frames):
+            th = [threading.Thread(target=worker, args=(i, frames)) for i in range(nthreads)]
+            for x in th:
+                x.start()
+            for x in th:
+                x.join()
+
+        run(CFRAMES * args.warmup)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local)
+        sampler.start()
+        t0 = time.perf_counter()
+        run(CFRAMES * args.steps)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        clocks = sampler.stop()
+        fps = nthreads * CFRAMES * args.steps / dt
+        sweep[nthreads] = round(fps, 2)
+        if best is None or fps > best[0]:
+            best = (fps, nthreads, dt, clocks, scores[0][-1])
+        ktimes = None
+        if not reference and nthreads == args.cvvdp_threads[0]:
+            h = handlers[0]
+            h.kernel_timing(True)
+            h.kernel_times(reset=True)
+            for f in range(CFRAMES):
+                a, b = host_pairs[f % len(host_pairs)]
+                h.compute(a, b, ls, ls)
+            kt = h.kernel_times(reset=True)
+            h.kernel_timing(False)
+            ktimes = {k: round(v[1] / CFRAMES, 4) for k, v in kt.items()}
+            sweep["kernels_ms_per_frame"] = ktimes
+        for h in handlers:
+            h.close()
+    for pb in pinned:
+        pb.free()
+    fps, nthreads, dt, clocks, last = best
+    line = {"metric": CMETRIC, "value": round(fps, 2), "unit": "frames/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": CWORKLOAD, "frames_per_step_per_sequence": CFRAMES, "width": W, "height": H,
+                       "display": "standard_fhd", "fps": 24.0, "sequences": nthreads, "threads_swept": sweep,
+                       "timer": "wall clock, synchronised"},
+            "e2e": {"value": round(fps, 2), "unit": "frames/s", "api": "Vship_ComputeCVVDP, pinned host frames",
+                    "h2d_bytes_per_step": nthreads * CFRAMES * input_bytes(pairs[:1]),
+                    "d2h_bytes_per_step": nthreads * CFRAMES * 8},
+            "last_jod": round(last, 6), "clocks": clocks}
+    if reference:
+        line["impl"] = "reference"
+        line["cpu_baseline"] = {"value": round(fps, 2), "unit": "frames/s", "kind": "reference", "cores": nthreads,
+                                "sample": "the reference has no CPU implementation: its own CUDA build on the B200"}
+        line["e2e"]["h2d_bytes_per_step"] = 0
+        line["e2e"]["d2h_bytes_per_step"] = 0
+    print(json.dumps(line), flush=True)
+
+
 UNEVEN_RES = [(640, 360), (1280, 720), (1920, 1080), (3840, 2160)]
 UNEVEN_N = 256
 UWORKLOAD = "ssimu2_uneven_256_srgb8_360p_720p_1080p_4k"
@@ -954,7 +1050,9 @@ def main():
     ap.add_argument("--ref-threads", type=int, nargs="+", default=[1, 3, 4, 8])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli", "ssimu2-uneven", "surrogate"],
+    ap.add_argument("--cvvdp-threads", type=int, nargs="+", default=[1, 2, 4],
+                    help="cvvdp: concurrent sequences (handlers) swept")
+    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli", "ssimu2-uneven", "surrogate", "cvvdp"],
                     help="butteraugli: secondary 4K Butteraugli line; ssimu2-uneven: 256 pairs of mixed "
                          "resolutions in one persistent launch, instead of the headline metric")
     ap.add_argument("--tile-rows", type=int, default=0, help="ssimu2-uneven: fixed map tile rows (0: autotune)")
@@ -984,6 +1082,10 @@ def main():
     if args.metric == "butteraugli":
         if args.impl == "ours" and rank == 0:
             run_butteraugli(args, world, rank, local)
+        return
+    if args.metric == "cvvdp":
+        if rank == 0:
+            run_cvvdp(args, rank, local, reference=args.impl == "reference")
         return
     if args.metric == "surrogate":
         if args.impl == "reference":

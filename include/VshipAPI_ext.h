@@ -200,6 +200,28 @@ EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateSetModel(VshipExt_SurrogateHa
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2Resolution(Vship_SSIMU2Handler handler, int64_t* width, int64_t* height);
 EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliResolution(Vship_ButteraugliHandler handler, int64_t* width, int64_t* height);
 
+/* ---- CVVDP display models (no reference counterpart) --------------------------------------
+ * The display a CVVDP handler would use for (model_key, model_config_json), resolved exactly as
+ * Vship_CVVDPInit2 resolves it (built-in model, then the JSON file's entry of that name), with
+ * the derived pixels per degree and black / reflected luminance.  Host only: needs no GPU.
+ * Errors: Vship_BadDisplayModel, Vship_BadPath, Vship_BadJson, Vship_BadPointer (null key or
+ * output), reported through the global last error. */
+typedef struct VshipExt_CVVDPDisplay {
+    int64_t width, height; /* resolution in pixels */
+    int hdr;               /* 0: SDR display (sRGB encoding), 1: HDR */
+    float viewing_distance_meters, diagonal_size_inches;
+    float max_luminance, contrast, E_ambient, k_refl, exposure;
+    float ppd;             /* pixels per visual degree */
+    float black_level;     /* max_luminance / contrast, cd/m^2 */
+    float reflected_level; /* E_ambient * k_refl / pi, cd/m^2 */
+} VshipExt_CVVDPDisplay;
+EXPORTPREPROCESS Vship_Exception VshipExt_CVVDPDisplayModel(const char* model_key, const char* model_config_json,
+                                                            VshipExt_CVVDPDisplay* out);
+/* Pyramid bands and ring length (frames) of a CVVDP handler. */
+EXPORTPREPROCESS Vship_Exception VshipExt_CVVDPGeometry(Vship_CVVDPHandler handler, int* bands, int* ring_frames);
+EXPORTPREPROCESS Vship_Exception VshipExt_CVVDPKernelTiming(Vship_CVVDPHandler handler, int enable);
+EXPORTPREPROCESS int VshipExt_CVVDPKernelTimes(Vship_CVVDPHandler handler, VshipExt_KernelTime* out, int max, int reset);
+
 #ifdef __cplusplus
 }
 #endif

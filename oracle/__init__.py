@@ -21,14 +21,15 @@ _lib = None
 
 def build(force=False):
     """Compile oracle.c (gcc, OpenMP).  Needs only gcc; runs here and on the GPU box."""
-    src = os.path.join(HERE, "oracle.c")
-    hdr = os.path.join(os.path.dirname(HERE), "vship_b200", "csrc", "metric_tables.h")
+    srcs = [os.path.join(HERE, "oracle.c"), os.path.join(HERE, "cvvdp.c")]
+    csrc = os.path.join(os.path.dirname(HERE), "vship_b200", "csrc")
+    deps = srcs + [os.path.join(csrc, "metric_tables.h"), os.path.join(csrc, "cvvdp_csf_table.h")]
     if (not force and os.path.exists(LIB_PATH)
-            and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(src), os.path.getmtime(hdr))):
+            and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(d) for d in deps)):
         return LIB_PATH
     tmp = LIB_PATH + ".tmp"
     subprocess.check_call(["gcc", "-O2", "-fopenmp", "-shared", "-fPIC", "-std=c11",
-                           "-fvisibility=hidden", "-o", tmp, src, "-lm"])
+                           "-fvisibility=hidden", "-o", tmp] + srcs + ["-lm"])
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 
@@ -59,6 +60,19 @@ def lib():
         L.oracle_downsample.argtypes = [dp, ctypes.c_int64, ctypes.c_int64, dp]
         L.oracle_positive_xyb.argtypes = [dp, ctypes.c_int64]
         L.oracle_num_threads.restype = ctypes.c_int
+        L.oracle_convert_native.argtypes = L.oracle_convert.argtypes
+        L.oracle_convert_native.restype = ctypes.c_int
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        L.oracle_cvvdp_new.restype = vp
+        L.oracle_cvvdp_new.argtypes = [i64, i64, ctypes.c_double, ctypes.c_int, dp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int]
+        L.oracle_cvvdp_free.argtypes = [vp]
+        L.oracle_cvvdp_info.argtypes = [vp, ctypes.POINTER(i64)]
+        L.oracle_cvvdp_filters.argtypes = [vp, dp]
+        L.oracle_cvvdp_reset.argtypes = [vp, ctypes.c_int]
+        L.oracle_cvvdp_frame.argtypes = [vp, dp, dp, ctypes.c_int, dp, dp]
+        L.oracle_cvvdp_bands.argtypes = [vp, dp]
+        L.oracle_cvvdp_bands.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -78,6 +92,87 @@ def convert(planes, line_sizes, cs):
     if rc != 0:
         raise ValueError("unsupported chroma subsampling")
     return out
+
+
+def convert_native(planes, line_sizes, cs):
+    """Like convert() but in the clip's own primaries (CVVDP's input, src/cvvdp/main.hpp:188)."""
+    ow, oh = cs.out_dims()
+    out = np.empty((3, oh, ow), dtype=np.float64)
+    bufs = [np.ascontiguousarray(np.frombuffer(memoryview(p), dtype=np.uint8)) for p in planes]
+    ptrs = (ctypes.c_void_p * 3)(*[b.ctypes.data for b in bufs])
+    ls = (ctypes.c_int64 * 3)(*line_sizes)
+    rc = lib().oracle_convert_native(ptrs, ls, ctypes.byref(cs), _dp(out))
+    if rc != 0:
+        raise ValueError("unsupported chroma subsampling")
+    return out
+
+
+# Built-in CVVDP displays (src/cvvdp/display_models.hpp:40-106) as oracle_cvvdp_new's model
+# vector: res_x, res_y, hdr, viewing distance (m), diagonal (in), peak luminance, contrast,
+# ambient illuminance (lux), k_refl, exposure.
+CVVDP_DISPLAYS = {
+    "standard_4k": (3840, 2160, 0, 0.7472, 30, 200, 1000, 250, 0.005, 1),
+    "standard_hdr_pq": (3840, 2160, 1, 0.7472, 30, 1500, 1000000, 10, 0.005, 1),
+    "standard_hdr_hlg": (3840, 2160, 1, 0.7472, 30, 1500, 1000000, 10, 0.005, 1),
+    "standard_hdr_linear": (3840, 2160, 1, 0.7472, 30, 1500, 1000000, 10, 0.005, 1),
+    "standard_hdr_dark": (3840, 2160, 1, 0.7472, 30, 1500, 1000000, 0, 0.005, 1),
+    "standard_hdr_linear_zoom": (3840, 2160, 1, 0.25, 30, 10000, 1000000, 10, 0.005, 1),
+    "standard_fhd": (1920, 1080, 0, 0.6, 24, 200, 1000, 250, 0.005, 1),
+}
+
+
+class CVVDP:
+    """FP64 CVVDP of one clip pair with the reference's temporal state (cvvdp.c)."""
+
+    def __init__(self, width, height, fps, display="standard_fhd", resize_to_display=False,
+                 trc=(abi.TRC_BT709, abi.TRC_BT709), primaries=(abi.PRIMARIES_BT709, abi.PRIMARIES_BT709)):
+        model = display if not isinstance(display, str) else CVVDP_DISPLAYS[display]
+        m = np.ascontiguousarray(model, dtype=np.float64)
+        self.h = lib().oracle_cvvdp_new(width, height, float(fps), 1 if resize_to_display else 0, _dp(m),
+                                        trc[0], primaries[0], trc[1], primaries[1])
+        if not self.h:
+            raise ValueError("frame too small for CVVDP")
+        info = (ctypes.c_int64 * 6)()
+        lib().oracle_cvvdp_info(self.h, info)
+        self.resize = (info[0], info[1])
+        self.levels, self.taps = info[2], info[3]
+
+    def frame(self, lin1, lin2, compute=True, distmap=False):
+        """lin1/lin2: (3, H, W) linear RGB in the clip primaries.  Returns the JOD score (and the
+        distortion map when asked) after adding the frame; None when compute is False."""
+        a = np.ascontiguousarray(lin1, dtype=np.float64)
+        b = np.ascontiguousarray(lin2, dtype=np.float64)
+        score = ctypes.c_double(0.0)
+        dmap = np.zeros((self.resize[1], self.resize[0]), dtype=np.float64) if distmap else None
+        lib().oracle_cvvdp_frame(self.h, _dp(a), _dp(b), 1 if compute else 0, ctypes.byref(score),
+                                 _dp(dmap) if distmap else None)
+        if not compute:
+            return None
+        return (score.value, dmap) if distmap else score.value
+
+    def bands(self):
+        vals = np.zeros(4 * self.levels, dtype=np.float64)
+        q = lib().oracle_cvvdp_bands(self.h, _dp(vals))
+        return vals.reshape(self.levels, 4), q
+
+    def filters(self):
+        out = np.zeros(4 * self.taps, dtype=np.float64)
+        lib().oracle_cvvdp_filters(self.h, _dp(out))
+        return out.reshape(4, self.taps)
+
+    def reset(self, only_score=False):
+        lib().oracle_cvvdp_reset(self.h, 1 if only_score else 0)
+
+    def close(self):
+        if self.h:
+            lib().oracle_cvvdp_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def ssimu2(rgb1, rgb2):

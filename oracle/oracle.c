@@ -276,7 +276,7 @@ static void primaries_to_709(double v[3], Vship_Primaries_t p) {
 /* horizontalResizeTranspose_Kernel (resize.hpp:26-48): cubic Hermite resize of each row
  * to rw samples, written transposed.  The source coordinate x*sw/rw is formed in float as
  * in the reference. */
-static void resize_transpose(const double* src, int64_t sw, int64_t sh, int64_t rw, double* dst) {
+void oracle_resize_transpose(const double* src, int64_t sw, int64_t sh, int64_t rw, double* dst) {
     #pragma omp parallel for
     for (int64_t y = 0; y < sh; y++) {
         for (int64_t x = 0; x < rw; x++) {
@@ -292,10 +292,12 @@ static void resize_transpose(const double* src, int64_t sw, int64_t sh, int64_t 
     }
 }
 
-/* Converter::convert (vshipColor.hpp:62-146): raw planes -> linear BT.709 RGB, planar,
- * at the final (resized, cropped) size.  Returns 0, or 1 for an unsupported subsampling. */
-ORACLE_API int oracle_convert(const uint8_t* const planes[3], const int64_t linesize[3],
-                              const Vship_Colorspace_t* cs, double* out) {
+/* Converter::convert (vshipColor.hpp:62-146): raw planes -> linear RGB, planar, at the
+ * final (resized, cropped) size; in BT.709 primaries (destination linRGBBT709), or in the
+ * clip's own primaries when `native` (destination linRGB, used by CVVDP,
+ * src/cvvdp/main.hpp:188).  Returns 0, or 1 for an unsupported subsampling. */
+static int convert_impl(const uint8_t* const planes[3], const int64_t linesize[3],
+                        const Vship_Colorspace_t* cs, int native, double* out) {
     const int64_t W = cs->width, H = cs->height;
     const int subw = cs->subsampling.subw, subh = cs->subsampling.subh;
     if (subw < 0 || subw > 2 || subh < 0 || subh > 1) return 1;
@@ -323,7 +325,7 @@ ORACLE_API int oracle_convert(const uint8_t* const planes[3], const int64_t line
             transfer(v, cs->transferFunction);
             linear_light(v, cs->YUVMatrix);
         }
-        primaries_to_709(v, cs->primaries);
+        if (!native) primaries_to_709(v, cs->primaries);
         full[i] = v[0]; full[N + i] = v[1]; full[2 * N + i] = v[2];
     }
     const int64_t TW = cs->target_width == -1 ? W : cs->target_width;
@@ -335,8 +337,8 @@ ORACLE_API int oracle_convert(const uint8_t* const planes[3], const int64_t line
         if (TW != W || TH != H) {
             double* tmp = (double*)malloc(sizeof(double) * TW * H);
             rs = (double*)malloc(sizeof(double) * TW * TH);
-            resize_transpose(src, W, H, TW, tmp);   /* -> TW rows of H */
-            resize_transpose(tmp, H, TW, TH, rs);   /* -> TH rows of TW */
+            oracle_resize_transpose(src, W, H, TW, tmp);   /* -> TW rows of H */
+            oracle_resize_transpose(tmp, H, TW, TH, rs);   /* -> TH rows of TW */
             free(tmp);
             src = rs;
         }
@@ -346,6 +348,16 @@ ORACLE_API int oracle_convert(const uint8_t* const planes[3], const int64_t line
     }
     free(full);
     return 0;
+}
+
+ORACLE_API int oracle_convert(const uint8_t* const planes[3], const int64_t linesize[3],
+                              const Vship_Colorspace_t* cs, double* out) {
+    return convert_impl(planes, linesize, cs, 0, out);
+}
+
+ORACLE_API int oracle_convert_native(const uint8_t* const planes[3], const int64_t linesize[3],
+                                     const Vship_Colorspace_t* cs, double* out) {
+    return convert_impl(planes, linesize, cs, 1, out);
 }
 
 /* ------------------------------------------------------------------------------------ */

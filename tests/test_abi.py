@@ -104,15 +104,19 @@ def test_invalid_handlers(vship_lib):
     assert "BadHandler" in buf.value.decode()
 
 
-def test_cvvdp_is_reported_missing(vship_lib):
+def test_cvvdp_host_errors(vship_lib):
+    """CVVDP entry points that fail before touching a device: NULL arguments and unknown ids."""
     L = vship_lib
     h = abi.CVVDPHandler()
     cs = abi.srgb8(8, 8)
     L.Vship_CVVDPInit.argtypes = [ctypes.POINTER(abi.CVVDPHandler), abi.Colorspace, abi.Colorspace,
                                   ctypes.c_float, ctypes.c_bool, ctypes.c_char_p]
-    assert L.Vship_CVVDPInit(ctypes.byref(h), cs, cs, 24.0, False, b"standard_4k") == abi.BadErrorType
+    assert L.Vship_CVVDPInit(ctypes.byref(h), cs, cs, 24.0, False, None) == abi.BadPointer
+    assert L.Vship_CVVDPInit(None, cs, cs, 24.0, False, b"standard_fhd") == abi.BadPointer
     L.Vship_ResetCVVDP.argtypes = [abi.CVVDPHandler]
-    assert L.Vship_ResetCVVDP(h) == abi.BadErrorType
+    assert L.Vship_ResetCVVDP(abi.CVVDPHandler(12345)) == abi.BadHandler
+    L.Vship_CVVDPFree.argtypes = [abi.CVVDPHandler]
+    assert L.Vship_CVVDPFree(abi.CVVDPHandler(12345)) == abi.BadHandler
 
 
 def test_struct_layouts_match_c():

@@ -34,6 +34,7 @@ EXCEPTIONS = {
 NoError, OutOfVRAM, OutOfRAM, HIPError = 0, 1, 2, 12
 DifferingInputType, DeviceCountError, NoDeviceDetected = 4, 6, 7
 BadDeviceArgument, BadDeviceCode, BadHandler, BadPointer, BadErrorType = 8, 9, 10, 11, 15
+BadDisplayModel, NonRGBSInput, BadPath, BadJson = 3, 5, 13, 14
 
 SAMPLE_BYTES = {SampleFLOAT: 4, SampleHALF: 2, SampleUINT8: 1, SampleUINT9: 2, SampleUINT10: 2,
                 SampleUINT12: 2, SampleUINT14: 2, SampleUINT16: 2}
@@ -123,6 +124,15 @@ class ButteraugliHandler(ctypes.Structure):
 
 class CVVDPHandler(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint)]
+
+
+class CVVDPDisplay(ctypes.Structure):
+    """VshipExt_CVVDPDisplay (include/VshipAPI_ext.h)."""
+    _fields_ = [("width", ctypes.c_int64), ("height", ctypes.c_int64), ("hdr", ctypes.c_int),
+                ("viewing_distance_meters", ctypes.c_float), ("diagonal_size_inches", ctypes.c_float),
+                ("max_luminance", ctypes.c_float), ("contrast", ctypes.c_float), ("E_ambient", ctypes.c_float),
+                ("k_refl", ctypes.c_float), ("exposure", ctypes.c_float), ("ppd", ctypes.c_float),
+                ("black_level", ctypes.c_float), ("reflected_level", ctypes.c_float)]
 
 
 class ButteraugliScore(ctypes.Structure):

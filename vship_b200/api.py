@@ -54,6 +54,20 @@ def _declare(L):
     L.Vship_ComputeButteraugli.argtypes = [HB, c.POINTER(abi.ButteraugliScore), c.c_void_p, c.c_int64, u8pp, u8pp, i64p, i64p]
     L.Vship_ButteraugliGetDetailedLastError.argtypes = [HB, c.c_char_p, c.c_int]
     L.Vship_ButteraugliGetDetailedLastError.restype = c.c_int
+    HC = abi.CVVDPHandler
+    L.Vship_CVVDPInit.argtypes = [c.POINTER(HC), abi.Colorspace, abi.Colorspace, c.c_float, c.c_bool, c.c_char_p]
+    L.Vship_CVVDPInit2.argtypes = [c.POINTER(HC), abi.Colorspace, abi.Colorspace, c.c_float, c.c_bool, c.c_char_p,
+                                   c.c_char_p]
+    L.Vship_CVVDPInit3.argtypes = [c.POINTER(HC), abi.Colorspace, abi.Colorspace, c.c_float, c.c_bool, c.c_char_p,
+                                   c.c_char_p, c.c_int]
+    L.Vship_CVVDPFree.argtypes = [HC]
+    L.Vship_CVVDPGetDistmapResolution.argtypes = [HC, i64p, i64p]
+    L.Vship_ResetCVVDP.argtypes = [HC]
+    L.Vship_ResetScoreCVVDP.argtypes = [HC]
+    L.Vship_LoadTemporalCVVDP.argtypes = [HC, u8pp, u8pp, i64p, i64p]
+    L.Vship_ComputeCVVDP.argtypes = [HC, c.POINTER(c.c_double), c.c_void_p, c.c_int64, u8pp, u8pp, i64p, i64p]
+    L.Vship_CVVDPGetDetailedLastError.argtypes = [HC, c.c_char_p, c.c_int]
+    L.Vship_CVVDPGetDetailedLastError.restype = c.c_int
     # extensions (absent from the reference library)
     if not hasattr(L, "VshipExt_ComputeSSIMU2Device"):
         return L
@@ -103,6 +117,11 @@ def _declare(L):
     L.VshipExt_SurrogateModel.argtypes = [HS, c.c_void_p, c.c_int]
     L.VshipExt_SurrogateModel.restype = c.c_int
     L.VshipExt_SurrogateSetModel.argtypes = [HS, c.c_void_p, c.c_int]
+    L.VshipExt_CVVDPDisplayModel.argtypes = [c.c_char_p, c.c_char_p, c.POINTER(abi.CVVDPDisplay)]
+    L.VshipExt_CVVDPGeometry.argtypes = [HC, c.POINTER(c.c_int), c.POINTER(c.c_int)]
+    L.VshipExt_CVVDPKernelTiming.argtypes = [HC, c.c_int]
+    L.VshipExt_CVVDPKernelTimes.argtypes = [HC, c.c_void_p, c.c_int, c.c_int]
+    L.VshipExt_CVVDPKernelTimes.restype = c.c_int
     return L
 
 
@@ -316,6 +335,105 @@ class Butteraugli:
             self.close()
         except Exception:
             pass
+
+
+class CVVDP:
+    """A CVVDP handler (Vship_CVVDPInit3 .. Vship_CVVDPFree): frames are fed in order; each
+    compute() returns the JOD of the sequence so far."""
+
+    def __init__(self, src_cs, dis_cs=None, fps=24.0, resize_to_display=False, model="standard_fhd",
+                 model_config_json=None, gpu_id=0, lib=None):
+        self.L = lib or load()
+        self.h = abi.CVVDPHandler()
+        self.src_cs, self.dis_cs = src_cs, dis_cs or src_cs
+        js = model_config_json.encode() if model_config_json else None
+        rc = self.L.Vship_CVVDPInit3(ctypes.byref(self.h), self.src_cs, self.dis_cs, float(fps), bool(resize_to_display),
+                                     model.encode(), js, gpu_id)
+        self.alive = True
+        if rc != 0:
+            msg = _message(self.L, self.L.Vship_CVVDPGetDetailedLastError, self.h)
+            self.close()
+            raise VshipError(rc, msg)
+
+    def _check(self, rc):
+        check(self.L, rc, self.L.Vship_CVVDPGetDetailedLastError, self.h)
+
+    def distmap_resolution(self):
+        w, h = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.L.Vship_CVVDPGetDistmapResolution(self.h, ctypes.byref(w), ctypes.byref(h)))
+        return w.value, h.value
+
+    def geometry(self):
+        """(pyramid bands, ring frames) -- extension."""
+        b, r = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.VshipExt_CVVDPGeometry(self.h, ctypes.byref(b), ctypes.byref(r)))
+        return b.value, r.value
+
+    def compute(self, planes1, planes2, line_sizes1, line_sizes2=None, distmap=False):
+        """Returns the JOD score, or (score, distortion map float32 (H, W)) with distmap."""
+        import numpy as np
+        a1, k1 = planes_arg(planes1)
+        a2, k2 = planes_arg(planes2)
+        ls1 = abi.LineSizes(*line_sizes1)
+        ls2 = abi.LineSizes(*(line_sizes2 or line_sizes1))
+        score = ctypes.c_double()
+        dm, dst, stride = None, None, 0
+        if distmap:
+            w, h = self.distmap_resolution()
+            dm = np.zeros((h, w), dtype=np.float32)
+            dst, stride = dm.ctypes.data, w * 4
+        self._check(self.L.Vship_ComputeCVVDP(self.h, ctypes.byref(score), dst, stride, a1, a2, ls1, ls2))
+        return (score.value, dm) if distmap else score.value
+
+    def load_temporal(self, planes1, planes2, line_sizes1, line_sizes2=None):
+        a1, k1 = planes_arg(planes1)
+        a2, k2 = planes_arg(planes2)
+        ls1 = abi.LineSizes(*line_sizes1)
+        ls2 = abi.LineSizes(*(line_sizes2 or line_sizes1))
+        self._check(self.L.Vship_LoadTemporalCVVDP(self.h, a1, a2, ls1, ls2))
+
+    def reset(self):
+        self._check(self.L.Vship_ResetCVVDP(self.h))
+
+    def reset_score(self):
+        self._check(self.L.Vship_ResetScoreCVVDP(self.h))
+
+    def kernel_timing(self, enable=True):
+        self._check(self.L.VshipExt_CVVDPKernelTiming(self.h, 1 if enable else 0))
+
+    def kernel_times(self, reset=False):
+        out = (KernelTime * 8)()
+        n = self.L.VshipExt_CVVDPKernelTimes(self.h, out, 8, 1 if reset else 0)
+        if n < 0:
+            check(self.L, abi.BadHandler)
+        return {out[i].name.decode(): (out[i].launches, out[i].total_ms) for i in range(n)}
+
+    def close(self):
+        if getattr(self, "alive", False):
+            self.alive = False
+            self.L.Vship_CVVDPFree(self.h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cvvdp_display(model="standard_fhd", model_config_json=None, lib=None):
+    """The display a CVVDP handler would use (VshipExt_CVVDPDisplayModel), as a dict; host only."""
+    L = lib or load()
+    out = abi.CVVDPDisplay()
+    js = model_config_json.encode() if model_config_json else None
+    rc = L.VshipExt_CVVDPDisplayModel(model.encode(), js, ctypes.byref(out))
+    check(L, rc)
+    return {f: getattr(out, f) for f, _ in abi.CVVDPDisplay._fields_}
 
 
 def frame_pairs(items):

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libvship.so")
 BUILD_DIR = os.path.join(HERE, "_build")
-SOURCES = ["api.cu", "ssimu2.cu", "ssimu2_batch.cu", "surrogate.cu", "butter.cu", "vsplugin.cu"]
+SOURCES = ["api.cu", "ssimu2.cu", "ssimu2_batch.cu", "surrogate.cu", "butter.cu", "cvvdp.cu", "vsplugin.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",

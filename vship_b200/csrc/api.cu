@@ -129,6 +129,7 @@ Table<Ssimu2Api> g_ssimu2;
 Table<ButterApi> g_butter;
 Table<Ssimu2BatchApi> g_batch;
 Table<SurrogateApi> g_surrogate;
+Table<CvvdpApi> g_cvvdp;
 
 template <typename EngineT>
 Vship_Exception fail(Slot<EngineT>* s, const Error& e) {
@@ -472,38 +473,78 @@ int Vship_ButteraugliGetDetailedLastError(Vship_ButteraugliHandler handler, char
     return handler_error(g_butter, handler.id, out_message, len, "Vship_ButteraugliGetDetailedLastError");
 }
 
-// ---------------------------------------------------------------- CVVDP (not provided)
+// ---------------------------------------------------------------- CVVDP
 
-static Vship_Exception cvvdp_missing(const char* where) {
-    set_global_error(Error(Vship_BadErrorType, __FILE__, __LINE__, std::string("CVVDP is not provided by this build (") + where + ")"));
-    return Vship_BadErrorType;
+Vship_Exception Vship_CVVDPInit3(Vship_CVVDPHandler* handler, Vship_Colorspace_t src, Vship_Colorspace_t dis, float fps,
+                                 bool resizeToDisplay, const char* model_key_cstr, const char* model_config_json_cstr,
+                                 int gpu_id) {
+    if (handler == nullptr || model_key_cstr == nullptr) {
+        set_global_error(Error(Vship_BadPointer, __FILE__, __LINE__, handler ? "model key is NULL" : "handler is NULL"));
+        return Vship_BadPointer;
+    }
+    const std::string key(model_key_cstr);
+    const std::string json(model_config_json_cstr ? model_config_json_cstr : "");
+    return init_handler(g_cvvdp, &handler->id, gpu_id, [&](Slot<CvvdpApi>& s) {
+        s.engine.reset(make_cvvdp_engine());
+        s.engine->init(src, dis, fps, resizeToDisplay, key, json, gpu_id);
+    });
 }
 
-Vship_Exception Vship_CVVDPInit(Vship_CVVDPHandler*, Vship_Colorspace_t, Vship_Colorspace_t, float, bool, const char*) {
-    return cvvdp_missing("Vship_CVVDPInit");
+Vship_Exception Vship_CVVDPInit2(Vship_CVVDPHandler* handler, Vship_Colorspace_t src, Vship_Colorspace_t dis, float fps,
+                                 bool resizeToDisplay, const char* model_key_cstr, const char* model_config_json_cstr) {
+    return Vship_CVVDPInit3(handler, src, dis, fps, resizeToDisplay, model_key_cstr, model_config_json_cstr, g_default_gpu);
 }
-Vship_Exception Vship_CVVDPInit2(Vship_CVVDPHandler*, Vship_Colorspace_t, Vship_Colorspace_t, float, bool, const char*, const char*) {
-    return cvvdp_missing("Vship_CVVDPInit2");
+
+Vship_Exception Vship_CVVDPInit(Vship_CVVDPHandler* handler, Vship_Colorspace_t src, Vship_Colorspace_t dis, float fps,
+                                bool resizeToDisplay, const char* model_key_cstr) {
+    return Vship_CVVDPInit2(handler, src, dis, fps, resizeToDisplay, model_key_cstr, nullptr);
 }
-Vship_Exception Vship_CVVDPInit3(Vship_CVVDPHandler*, Vship_Colorspace_t, Vship_Colorspace_t, float, bool, const char*, const char*, int) {
-    return cvvdp_missing("Vship_CVVDPInit3");
+
+Vship_Exception Vship_CVVDPFree(Vship_CVVDPHandler handler) { return free_handler(g_cvvdp, handler.id, "Vship_CVVDPFree"); }
+
+Vship_Exception Vship_CVVDPGetDistmapResolution(Vship_CVVDPHandler handler, int64_t* width, int64_t* height) {
+    return with_handler(g_cvvdp, handler.id, "Vship_CVVDPGetDistmapResolution", [&](Slot<CvvdpApi>& s) {
+        require_engine((bool)s.engine);
+        if (width) *width = s.engine->distmap_width();
+        if (height) *height = s.engine->distmap_height();
+    });
 }
-Vship_Exception Vship_CVVDPFree(Vship_CVVDPHandler) { return cvvdp_missing("Vship_CVVDPFree"); }
-Vship_Exception Vship_CVVDPGetDistmapResolution(Vship_CVVDPHandler, int64_t*, int64_t*) {
-    return cvvdp_missing("Vship_CVVDPGetDistmapResolution");
+
+Vship_Exception Vship_ResetCVVDP(Vship_CVVDPHandler handler) {
+    return with_handler(g_cvvdp, handler.id, "Vship_ResetCVVDP", [&](Slot<CvvdpApi>& s) {
+        require_engine((bool)s.engine);
+        s.engine->reset(false);
+    });
 }
-Vship_Exception Vship_ResetCVVDP(Vship_CVVDPHandler) { return cvvdp_missing("Vship_ResetCVVDP"); }
-Vship_Exception Vship_ResetScoreCVVDP(Vship_CVVDPHandler) { return cvvdp_missing("Vship_ResetScoreCVVDP"); }
-Vship_Exception Vship_LoadTemporalCVVDP(Vship_CVVDPHandler, const uint8_t*[3], const uint8_t*[3], const int64_t[3], const int64_t[3]) {
-    return cvvdp_missing("Vship_LoadTemporalCVVDP");
+
+Vship_Exception Vship_ResetScoreCVVDP(Vship_CVVDPHandler handler) {
+    return with_handler(g_cvvdp, handler.id, "Vship_ResetScoreCVVDP", [&](Slot<CvvdpApi>& s) {
+        require_engine((bool)s.engine);
+        s.engine->reset(true);
+    });
 }
-Vship_Exception Vship_ComputeCVVDP(Vship_CVVDPHandler, double*, const uint8_t*, int64_t, const uint8_t*[3], const uint8_t*[3],
-                                   const int64_t[3], const int64_t[3]) {
-    return cvvdp_missing("Vship_ComputeCVVDP");
+
+Vship_Exception Vship_LoadTemporalCVVDP(Vship_CVVDPHandler handler, const uint8_t* srcp1[3], const uint8_t* srcp2[3],
+                                        const int64_t lineSize[3], const int64_t lineSize2[3]) {
+    return with_handler(g_cvvdp, handler.id, "Vship_LoadTemporalCVVDP", [&](Slot<CvvdpApi>& s) {
+        require_engine((bool)s.engine);
+        if (!srcp1 || !srcp2 || !lineSize || !lineSize2) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        s.engine->load_temporal(srcp1, srcp2, lineSize, lineSize2);
+    });
 }
-int Vship_CVVDPGetDetailedLastError(Vship_CVVDPHandler, char*, int) {
-    cvvdp_missing("Vship_CVVDPGetDetailedLastError");
-    return 0;
+
+Vship_Exception Vship_ComputeCVVDP(Vship_CVVDPHandler handler, double* score, const uint8_t* dstp, int64_t dststride,
+                                   const uint8_t* srcp1[3], const uint8_t* srcp2[3], const int64_t lineSize[3],
+                                   const int64_t lineSize2[3]) {
+    return with_handler(g_cvvdp, handler.id, "Vship_ComputeCVVDP", [&](Slot<CvvdpApi>& s) {
+        require_engine((bool)s.engine);
+        if (!score || !srcp1 || !srcp2 || !lineSize || !lineSize2) throw Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument");
+        *score = s.engine->compute(const_cast<uint8_t*>(dstp), dststride, srcp1, srcp2, lineSize, lineSize2);
+    });
+}
+
+int Vship_CVVDPGetDetailedLastError(Vship_CVVDPHandler handler, char* out_message, int len) {
+    return handler_error(g_cvvdp, handler.id, out_message, len, "Vship_CVVDPGetDetailedLastError");
 }
 
 // ---------------------------------------------------------------- extensions
@@ -575,6 +616,39 @@ Vship_Exception VshipExt_ButteraugliResolution(Vship_ButteraugliHandler handler,
         if (width) *width = s.engine->width();
         if (height) *height = s.engine->height();
     });
+}
+
+Vship_Exception VshipExt_CVVDPDisplayModel(const char* model_key, const char* model_config_json, VshipExt_CVVDPDisplay* out) {
+    if (model_key == nullptr || out == nullptr) {
+        set_global_error(Error(Vship_BadPointer, __FILE__, __LINE__, "NULL argument"));
+        return Vship_BadPointer;
+    }
+    try {
+        cvvdp_display_model(model_key, model_config_json ? model_config_json : "", out);
+    } catch (const Error& e) {
+        set_global_error(e);
+        return e.code;
+    }
+    return Vship_NoError;
+}
+
+Vship_Exception VshipExt_CVVDPGeometry(Vship_CVVDPHandler handler, int* bands, int* ring_frames) {
+    return with_handler(g_cvvdp, handler.id, "VshipExt_CVVDPGeometry", [&](Slot<CvvdpApi>& s) {
+        require_engine((bool)s.engine);
+        if (bands) *bands = s.engine->bands();
+        if (ring_frames) *ring_frames = s.engine->ring_frames();
+    });
+}
+
+Vship_Exception VshipExt_CVVDPKernelTiming(Vship_CVVDPHandler handler, int enable) {
+    return with_handler(g_cvvdp, handler.id, "VshipExt_CVVDPKernelTiming", [&](Slot<CvvdpApi>& s) {
+        require_engine((bool)s.engine);
+        s.engine->timer().enable(enable != 0);
+    });
+}
+
+int VshipExt_CVVDPKernelTimes(Vship_CVVDPHandler handler, VshipExt_KernelTime* out, int max, int reset) {
+    return kernel_times(g_cvvdp, handler.id, out, max, reset);
 }
 
 // ---------------------------------------------------------------- uneven batches

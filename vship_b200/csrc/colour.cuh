@@ -444,18 +444,46 @@ __device__ __forceinline__ float2 chroma_from_stage(const ChromaStage& st, const
     return make_float2(out[0], out[1]);
 }
 
-// Y'CbCr (or R'G'B') -> linear BT.709 RGB of one pixel.
-__device__ __forceinline__ float3 to_linear_709(float3 v, const ColourParams& cp) {
+// Y'CbCr (or R'G'B') -> linear RGB of one pixel in the clip's own primaries (the
+// reference's linRGB destination, src/gpuColorToLinear/vshipColor.hpp:111-113).
+__device__ __forceinline__ float3 to_linear_native(float3 v, const ColourParams& cp) {
     if (!cp.skip_yuv) {
         v = gamma_light(v, cp.matrix);
         v = transfer(v, cp.trc);
         v = linear_light(v, cp.matrix);
     }
-    return primaries_to_709(v, cp.primaries);
+    return v;
 }
 
-// Linear BT.709 RGB of luma (X, Y) inside the tile with origin (X0, Y0) prepared by
-// chroma_stage (or of any pixel when the clip is not chroma-subsampled).
+// Y'CbCr (or R'G'B') -> linear BT.709 RGB of one pixel.
+__device__ __forceinline__ float3 to_linear_709(float3 v, const ColourParams& cp) {
+    return primaries_to_709(to_linear_native(v, cp), cp.primaries);
+}
+
+// Linear RGB in primaries `prim` -> CIE XYZ (primariesToPrimaries_device<P, INTERNAL>,
+// src/gpuColorToLinear/primaries.hpp:17-112).
+__device__ __forceinline__ float3 rgb_to_xyz(float3 v, int prim) {
+    switch (prim) {
+    case Vship_PRIMARIES_BT709:
+        return mat3f(v, 0.4124f, 0.3576f, 0.1805f, 0.2126f, 0.7152f, 0.0722f, 0.0193f, 0.1192f, 0.9505f);
+    case Vship_PRIMARIES_BT2020:
+        return mat3f(v, 0.6370f, 0.1446f, 0.1689f, 0.2627f, 0.6780f, 0.0593f, 0.f, 0.0281f, 1.0610f);
+    case Vship_PRIMARIES_ST170_M:
+    case Vship_PRIMARIES_ST240_M:
+        return mat3f(v, 0.39349893f, 0.3652766f, 0.19162447f, 0.2123645f, 0.70109542f, 0.08654008f, 0.01873804f, 0.1119396f, 0.95812235f);
+    case Vship_PRIMARIES_BT470_BG:
+        return mat3f(v, 0.4305f, 0.3416f, 0.1783f, 0.2220f, 0.7067f, 0.07132f, 0.0202f, 0.1296f, 0.9391f);
+    case Vship_PRIMARIES_BT470_M:
+        return mat3f(v, 0.6068f, 0.1735f, 0.2003f, 0.2989f, 0.5866f, 0.1145f, 0.f, 0.06609f, 1.116f);
+    default:
+        return v;  // INTERNAL: already XYZ
+    }
+}
+
+// Linear RGB of luma (X, Y) inside the tile with origin (X0, Y0) prepared by chroma_stage
+// (or of any pixel when the clip is not chroma-subsampled): BT.709 primaries, or the clip's
+// own primaries when kNative.
+template <bool kNative = false>
 __device__ __forceinline__ float3 ingest_staged(const RawImage& im, const ColourParams& cp, const ChromaStage& st,
                                                int X, int Y, int X0, int Y0) {
     float3 v;
@@ -469,7 +497,7 @@ __device__ __forceinline__ float3 ingest_staged(const RawImage& im, const Colour
         v.y = c.x;
         v.z = c.y;
     }
-    return to_linear_709(v, cp);
+    return kNative ? to_linear_native(v, cp) : to_linear_709(v, cp);
 }
 
 // Linear BT.709 RGB of luma position (X, Y) of one raw image.

@@ -90,7 +90,33 @@ struct SurrogateApi {
     virtual KernelTimer& timer() = 0;
 };
 
+// CVVDP engine of one handler (replaces cvvdp::CVVDPComputingImplementation,
+// src/cvvdp/main.hpp:161-398): a ring of past frames per clip and the running temporal score.
+struct CvvdpApi {
+    virtual ~CvvdpApi() = default;
+    virtual void init(const Vship_Colorspace_t& src, const Vship_Colorspace_t& dis, float fps, bool resize_to_display,
+                      const std::string& model_key, const std::string& model_config_json, int device) = 0;
+    // Adds a frame pair to the ring, scores it and returns the JOD of the sequence so far;
+    // dstp (nullable) receives the distortion map (rows of dststride bytes).
+    virtual double compute(uint8_t* dstp, int64_t dststride, const uint8_t* const s1[3], const uint8_t* const s2[3],
+                           const int64_t ls1[3], const int64_t ls2[3]) = 0;
+    // Adds a frame pair to the ring without scoring it.
+    virtual void load_temporal(const uint8_t* const s1[3], const uint8_t* const s2[3], const int64_t ls1[3],
+                               const int64_t ls2[3]) = 0;
+    // Empties the ring and the score (only_score: the score only).
+    virtual void reset(bool only_score) = 0;
+    virtual int64_t distmap_width() const = 0;
+    virtual int64_t distmap_height() const = 0;
+    virtual int bands() const = 0;
+    virtual int ring_frames() const = 0;
+    virtual KernelTimer& timer() = 0;
+};
+
+// Resolves a CVVDP display model (built-in name, then the JSON file's entry); throws Error.
+void cvvdp_display_model(const std::string& model_key, const std::string& model_config_json, VshipExt_CVVDPDisplay* out);
+
 Ssimu2Api* make_ssimu2_engine();
+CvvdpApi* make_cvvdp_engine();
 SurrogateApi* make_surrogate_engine();
 Ssimu2BatchApi* make_ssimu2_batch_engine();
 void record_global_error(const Error& e);

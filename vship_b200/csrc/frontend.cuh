@@ -206,8 +206,10 @@ inline bool misaligned_view(const RawImage& im, const ClipGeometry& g) {
 // ---- generic path: ingest to planar linear RGB, then resize (horizontalResizeTranspose,
 // ---- src/gpuColorToLinear/resize.hpp:26-48), crop by offset.
 
-// Planar linear RGB of one image, one 64x64 luma tile per CTA with its chroma staged in
-// shared memory (dynamic: chroma_stage_floats(subw, subh) floats).
+// Planar linear RGB of one image (BT.709 primaries, or the clip's own when kNative), one
+// 64x64 luma tile per CTA with its chroma staged in shared memory (dynamic:
+// chroma_stage_floats(subw, subh) floats).
+template <bool kNative>
 static __global__ void __launch_bounds__(256) ingest_linear_kernel(RawImage im, ColourParams cp, float* out, int64_t plane_stride) {
     extern __shared__ float stage_mem[];
     const int X0 = blockIdx.x * kStageTile, Y0 = blockIdx.y * kStageTile;
@@ -216,7 +218,7 @@ static __global__ void __launch_bounds__(256) ingest_linear_kernel(RawImage im, 
     for (int i = threadIdx.x; i < kStageTile * kStageTile; i += blockDim.x) {
         const int X = X0 + (i & (kStageTile - 1)), Y = Y0 + i / kStageTile;
         if (X >= cp.W || Y >= cp.H) continue;
-        const float3 v = ingest_staged(im, cp, st, X, Y, X0, Y0);
+        const float3 v = ingest_staged<kNative>(im, cp, st, X, Y, X0, Y0);
         const int64_t o = (int64_t)Y * cp.W + X;
         out[o] = v.x;
         out[plane_stride + o] = v.y;
@@ -224,11 +226,13 @@ static __global__ void __launch_bounds__(256) ingest_linear_kernel(RawImage im, 
     }
 }
 
-inline void launch_ingest_linear(const RawImage& im, const ColourParams& cp, float* out, int64_t plane_stride, cudaStream_t st) {
+inline void launch_ingest_linear(const RawImage& im, const ColourParams& cp, float* out, int64_t plane_stride, cudaStream_t st,
+                                 bool native = false) {
     const dim3 grid((unsigned)ceil_div(cp.W, kStageTile), (unsigned)ceil_div(cp.H, kStageTile));
     const size_t smem = sizeof(float) * chroma_stage_floats(cp.subw, cp.subh);
-    if (smem > 48 * 1024) CUDA_CHECK(cudaFuncSetAttribute(ingest_linear_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    ingest_linear_kernel<<<grid, 256, smem, st>>>(im, cp, out, plane_stride);
+    auto kernel = native ? ingest_linear_kernel<true> : ingest_linear_kernel<false>;
+    if (smem > 48 * 1024) CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kernel<<<grid, 256, smem, st>>>(im, cp, out, plane_stride);
     CUDA_CHECK(cudaGetLastError());
 }
 
@@ -265,11 +269,11 @@ struct GenericLinear {
         device_free(scratch);
         planes = scratch = nullptr;
     }
-    void run(const RawImage& im, const ColourParams& cp, const ClipGeometry& g, cudaStream_t stream) {
+    void run(const RawImage& im, const ColourParams& cp, const ClipGeometry& g, cudaStream_t stream, bool native = false) {
         const int64_t n = g.W * g.H;
         float* lin = g.resized ? scratch : planes;
         const int64_t lin_stride = g.resized ? n : plane_floats;
-        launch_ingest_linear(im, cp, lin, lin_stride, stream);
+        launch_ingest_linear(im, cp, lin, lin_stride, stream, native);
         if (!g.resized) return;
         float* mid = scratch + 3 * n;
         for (int c = 0; c < 3; c++) {
