@@ -8,10 +8,12 @@
 //                 Y transient at pyramid level 0 (temporalFilter.hpp:150-193)
 //   cv_reduce     one Gaussian pyramid step of all eight planes (two clips x four
 //                 channels) per launch (lpyr.hpp:7-36)
-//   cv_band       one Laplacian band: expansion of the next level, contrast against the
-//                 background luminance, CSF weighting, the sigma-3 masking blur, cross-channel
-//                 masking, the saturating D and per-tile FP64 sums of D^2; one 32x32 tile per
-//                 CTA (lpyr.hpp:177-236, csf.hpp, maskingModel.hpp:5-96)
+//   cv_contrast   one Laplacian band of both clips: expansion of the next level, contrast
+//                 against the background luminance, CSF weighting; writes the masking input
+//                 min(|R|,|T|) and |R-T| per channel (lpyr.hpp:177-236, csf.hpp,
+//                 maskingModel.hpp:5-15)
+//   cv_mask       the sigma-3 masking blur, cross-channel masking, the saturating D and
+//                 per-tile FP64 sums of D^2; one 32x32 tile per CTA (maskingModel.hpp:28-96)
 //   cv_baseband   the baseband: mean luminance, contrast, D and its pooled norm in one CTA
 //                 (lpyr.hpp:219-229, maskingModel.hpp:106-114)
 //   cv_final      pooled norm of every band and channel (pooling.hpp)
@@ -307,20 +309,103 @@ __device__ __forceinline__ float sensitivity(const float* col, float lum0, float
     return exp10f(logs);
 }
 
-// ---- one Laplacian band ------------------------------------------------------------------
+// ---- one Laplacian band: contrast and CSF ------------------------------------------------
 
-constexpr int kBT = 32;               // output tile
-constexpr int kBH = 8;                // masking blur radius
-constexpr int kBI = kBT + 2 * kBH;    // 48: tile with halo
-constexpr int kBandThreads = 256;
+// Positive x to the power g through the hardware base-2 exponential and logarithm
+// (relative error about 1e-6); 0 for x <= 0.
+__device__ __forceinline__ float pow_pos(float x, float g) { return x > 0.f ? ex2_approx(g * __log2f(x)) : 0.f; }
 
-struct BandParams {
+constexpr int kCW = 64;                   // contrast tile: 64 x 16 pixels of the band
+constexpr int kCHt = 16;
+constexpr int kCoarseW = kCW / 2 + 2;     // 34 coarse columns feed it (expansion taps)
+constexpr int kCoarseH = kCHt / 2 + 2;    // 10 coarse rows
+constexpr int kContrastThreads = 256;
+
+struct ContrastParams {
     const float* g[2][4];   // level b planes (w x h)
     const float* gn[2][4];  // level b+1 planes
     int w, h, tiles_x;
     float mult;             // contrast multiplier: 1 at band 0, 2 below
     const float* csf;       // 4 x 32 log10 sensitivities of this band
     float lum0, span;       // log10 of the first luminance sample and the axis span
+    float* mn[4];           // out: min(|R|, |T|) per channel (w x h)
+    float* df[4];           // out: |R - T| per channel
+};
+
+// Laplacian layer of both clips (G_b - expand(G_b+1), the Y channel against the clamped
+// background; lpyr.hpp:177-215), contrast against the background luminance, CSF weighting by
+// the reference clip's background (preGaussianPreCompute_kernel, maskingModel.hpp:5-15).
+// The tile's coarse neighbourhood of all eight next-level planes is staged in shared memory
+// with the expansion's mirror padding already applied.
+__global__ void __launch_bounds__(kContrastThreads) cv_contrast_kernel(const __grid_constant__ ContrastParams p) {
+    __shared__ float coarse[8][kCoarseH][kCoarseW];
+    __shared__ float csf[4][32];
+    const int tid = threadIdx.x;
+    const int X0 = (blockIdx.x % p.tiles_x) * kCW, Y0 = (blockIdx.x / p.tiles_x) * kCHt;
+    const int ow = (p.w + 1) / 2, oh = (p.h + 1) / 2;
+    const int cx0 = X0 / 2 - 1, cy0 = Y0 / 2 - 1;
+    if (tid < 128) csf[tid >> 5][tid & 31] = p.csf[tid];
+    for (int i = tid; i < 8 * kCoarseH * kCoarseW; i += kContrastThreads) {
+        const int q = i / (kCoarseH * kCoarseW), r = (i / kCoarseW) % kCoarseH, c = i % kCoarseW;
+        int rx = cx0 + c, ry = cy0 + r;
+        if (rx < 0) rx = -rx - 1;
+        if (rx >= ow) rx = 2 * ow - rx - 2;
+        if (ry < 0) ry = -ry - 1;
+        if (ry >= oh) ry = 2 * oh - ry - 2;
+        rx = min(max(rx, 0), ow - 1);  // only pixels past the band edge reach beyond the mirror
+        ry = min(max(ry, 0), oh - 1);
+        coarse[q][r][c] = __ldg(p.gn[q >> 2][q & 3] + (int64_t)ry * ow + rx);
+    }
+    __syncthreads();
+    for (int i = tid; i < kCW * kCHt; i += kContrastThreads) {
+        const int x = X0 + (i % kCW), y = Y0 + i / kCW;
+        if (x >= p.w || y >= p.h) continue;
+        const int px = x & 1, py = y & 1;
+        const int ix0 = (x - X0 - 2 + px) / 2 + 1, iy0 = (y - Y0 - 2 + py) / 2 + 1;  // first taps
+        float e[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) e[q] = 0.f;
+        for (int ty = 0; ty < 3 - py; ty++) {
+            const float ky = 2.f * pyr_k(2 * ty - 2 + py + 2);
+            for (int tx = 0; tx < 3 - px; tx++) {
+                const float k = (2.f * pyr_k(2 * tx - 2 + px + 2)) * ky;
+#pragma unroll
+                for (int q = 0; q < 8; q++) e[q] = fmaf(k, coarse[q][iy0 + ty][ix0 + tx], e[q]);
+            }
+        }
+        const int64_t j = (int64_t)y * p.w + x;
+        float con[2][4];
+        float lref = 0.f;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float lb = fmaxf(e[4 * k], 0.01f);
+            if (k == 0) lref = lb;
+            const float inv = 1.f / lb;
+            con[k][0] = fminf((__ldg(p.g[k][0] + j) - lb) * inv, 1000.f) * p.mult;
+#pragma unroll
+            for (int c = 1; c < 4; c++) con[k][c] = fminf((__ldg(p.g[k][c] + j) - e[4 * k + c]) * inv, 1000.f) * p.mult;
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float s = sensitivity(csf[c], p.lum0, p.span, lref) * (c == 1 ? 1.45f : 1.f);
+            const float r = con[0][c] * s, t = con[1][c] * s;
+            p.mn[c][j] = fminf(fabsf(r), fabsf(t));
+            p.df[c][j] = fabsf(r - t);
+        }
+    }
+}
+
+// ---- one Laplacian band: masking and D ---------------------------------------------------
+
+constexpr int kBT = 32;               // output tile
+constexpr int kBH = 8;                // masking blur radius
+constexpr int kBI = kBT + 2 * kBH;    // 48: tile with halo
+constexpr int kBandThreads = 256;
+
+struct MaskParams {
+    const float* mn[4];
+    const float* df[4];
+    int w, h, tiles_x;
     float blur_w[17];
     float blur_prefix[18];
     float xcm2[16];         // 2^xcm_weights[k * 4 + c]
@@ -329,65 +414,30 @@ struct BandParams {
     float merge_div;
 };
 
-struct BandSmem {
-    float mn[4][kBI][kBI];     // min(|R|, |T|) over the tile and its halo (0 outside the plane)
+struct MaskSmem {
+    float mn[4][kBI][kBI];     // masking input over the tile and its halo (0 outside the plane)
     float hb[4][kBI][kBT];     // horizontally blurred
-    float diff[4][kBT][kBT];   // |R - T| at the tile's pixels
-    float csf[4][32];
     float prefix[18];          // cumulative blur weights, for the in-plane renormalisation
     double red[kBandThreads / 32][4];
 };
 
-__global__ void __launch_bounds__(kBandThreads) cv_band_kernel(const __grid_constant__ BandParams p) {
-    extern __shared__ __align__(16) unsigned char band_smem_raw[];
-    BandSmem& sm = *reinterpret_cast<BandSmem*>(band_smem_raw);
+// The sigma-3 renormalised blur of min(|R|, |T|) (GaussianSmart_Device, gaussianBlur.hpp:62-119),
+// cross-channel masking, the saturating D with the channel weights (computeD_Kernel,
+// maskingModel.hpp:28-96), the tile's FP64 sums of D^2 and, for the distortion map, the
+// 4-norm over channels (mergeChromaNorm_Kernel, distmap_specifics.hpp:27-33).
+__global__ void __launch_bounds__(kBandThreads) cv_mask_kernel(const __grid_constant__ MaskParams p) {
+    extern __shared__ __align__(16) unsigned char mask_smem_raw[];
+    MaskSmem& sm = *reinterpret_cast<MaskSmem*>(mask_smem_raw);
     const int tid = threadIdx.x;
     const int X0 = (blockIdx.x % p.tiles_x) * kBT, Y0 = (blockIdx.x / p.tiles_x) * kBT;
-    if (tid < 128) sm.csf[tid >> 5][tid & 31] = p.csf[tid];
     if (tid < 18) sm.prefix[tid] = p.blur_prefix[tid];
-    __syncthreads();
-    const float powmaskc = exp10f(kMaskC);
-
-    // Contrast of both clips, CSF weighting (preGaussianPreCompute_kernel), masking input.
-    for (int i = tid; i < kBI * kBI; i += kBandThreads) {
-        const int ry = i / kBI, rx = i - ry * kBI;
-        const int gx = X0 - kBH + rx, gy = Y0 - kBH + ry;
+    for (int i = tid; i < 4 * kBI * kBI; i += kBandThreads) {
+        const int c = i / (kBI * kBI), r = (i / kBI) % kBI, x = i % kBI;
+        const int gx = X0 - kBH + x, gy = Y0 - kBH + r;
         const bool in = gx >= 0 && gx < p.w && gy >= 0 && gy < p.h;
-        const bool centre = rx >= kBH && rx < kBH + kBT && ry >= kBH && ry < kBH + kBT;
-        if (!in) {
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                sm.mn[c][ry][rx] = 0.f;
-                if (centre) sm.diff[c][ry - kBH][rx - kBH] = 0.f;
-            }
-            continue;
-        }
-        const int64_t j = (int64_t)gy * p.w + gx;
-        float con[2][4];
-        float lref = 0.f;
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const float lb = fmaxf(pyr_expand(p.gn[k][0], p.w, p.h, gx, gy), 0.01f);
-            if (k == 0) lref = lb;
-            con[k][0] = fminf((__ldg(p.g[k][0] + j) - lb) / lb, 1000.f) * p.mult;
-#pragma unroll
-            for (int c = 1; c < 4; c++) {
-                const float layer = __ldg(p.g[k][c] + j) - pyr_expand(p.gn[k][c], p.w, p.h, gx, gy);
-                con[k][c] = fminf(layer / lb, 1000.f) * p.mult;
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const float s = sensitivity(sm.csf[c], p.lum0, p.span, lref) * (c == 1 ? 1.45f : 1.f);
-            const float r = con[0][c] * s, t = con[1][c] * s;
-            sm.mn[c][ry][rx] = fminf(fabsf(r), fabsf(t));
-            if (centre) sm.diff[c][ry - kBH][rx - kBH] = fabsf(r - t);
-        }
+        sm.mn[c][r][x] = in ? __ldg(p.mn[c] + (int64_t)gy * p.w + gx) : 0.f;
     }
     __syncthreads();
-
-    // Horizontal pass of the renormalised sigma-3 blur (GaussianSmart_Device,
-    // gaussianBlur.hpp:62-119): 48 rows x 32 columns x 4 channels.
     for (int i = tid; i < 4 * kBI * kBT; i += kBandThreads) {
         const int c = i / (kBI * kBT);
         const int r = (i / kBT) % kBI;
@@ -405,8 +455,7 @@ __global__ void __launch_bounds__(kBandThreads) cv_band_kernel(const __grid_cons
         sm.hb[c][r][x] = v;
     }
     __syncthreads();
-
-    // Vertical pass, masking and D (computeD_Kernel, maskingModel.hpp:28-96).
+    const float powmaskc = exp10f(kMaskC);
     const float max_v = exp10f(kDMax);
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = tid; i < kBT * kBT; i += kBandThreads) {
@@ -416,26 +465,27 @@ __global__ void __launch_bounds__(kBandThreads) cv_band_kernel(const __grid_cons
         const int beg = max(0, gy - 8) - (gy - 8);   // 0..8
         const int end = min(p.h, gy + 9) - (gy - 8);  // 9..17
         const float inv = 1.f / (sm.prefix[end] - sm.prefix[beg]);
+        const int64_t j = (int64_t)gy * p.w + gx;
         float cm[4];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             float s = 0.f;
 #pragma unroll
             for (int t = 0; t < 17; t++) s = fmaf(sm.hb[c][y + t][x], p.blur_w[t], s);
-            cm[c] = powf(powmaskc * fabsf(s * inv), kMaskQ[c]);
+            cm[c] = pow_pos(powmaskc * fabsf(s * inv), kMaskQ[c]);
         }
         float d[4];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const float cmask = fmaf(cm[0], p.xcm2[c], fmaf(cm[1], p.xcm2[4 + c], fmaf(cm[2], p.xcm2[8 + c], cm[3] * p.xcm2[12 + c])));
-            const float du = powf(sm.diff[c][y][x], kMaskP) / (1.f + cmask);
+            const float du = pow_pos(__ldg(p.df[c] + j), kMaskP) / (1.f + cmask);
             d[c] = max_v * du / (max_v + du) * (c == 3 ? kChTransW : 1.f);
             acc[c] += (double)d[c] * (double)d[c];
         }
         if (p.merged) {
             const float q = (d[0] * d[0]) * (d[0] * d[0]) + (d[1] * d[1]) * (d[1] * d[1]) + (d[2] * d[2]) * (d[2] * d[2]) +
                             (d[3] * d[3]) * (d[3] * d[3]);
-            p.merged[(int64_t)gy * p.w + gx] = powf(q * 0.25f, 0.25f) / p.merge_div;
+            p.merged[j] = pow_pos(q * 0.25f, 0.25f) / p.merge_div;
         }
     }
 #pragma unroll
@@ -961,7 +1011,7 @@ public:
         CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         CUDA_CHECK(cudaEventCreateWithFlags(&last_done_, cudaEventDisableTiming));
         // per device: the caller has selected this handler's device
-        CUDA_CHECK(cudaFuncSetAttribute(cv_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BandSmem)));
+        CUDA_CHECK(cudaFuncSetAttribute(cv_mask_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MaskSmem)));
         for (int k = 0; k < 2; k++) {
             int64_t po[3];
             staging_[k].ensure((size_t)dense_image_bytes(geo_[k], po), stream_);
@@ -971,6 +1021,7 @@ public:
         const int64_t mn = mw_ * mh_;
         ring_ = device_alloc<float>((size_t)(2 * (int64_t)taps_ * 3 * mn), "temporal ring");
         pyr_ = device_alloc<float>((size_t)(2 * 4 * chan_stride_), "contrast pyramid");
+        if (levels_ > 1) mask_buf_ = device_alloc<float>((size_t)(8 * rw_ * rh_), "band masking planes");
         if (mw_ < rw_) up_buf_ = device_alloc<float>((size_t)(2 * 4 * mn + rw_ * mh_), "upscale planes");
         filt_d_ = device_alloc<float>(filt.size(), "temporal filters");
         CUDA_CHECK(cudaMemcpy(filt_d_, filt.data(), filt.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -1163,26 +1214,38 @@ private:
 
         t = timer_.begin(3, "cvvdp_band", stream_);
         for (int b = 0; b + 1 < levels_; b++) {
-            BandParams bp{};
+            ContrastParams cp{};
+            MaskParams mp{};
             for (int k = 0; k < 2; k++)
                 for (int c = 0; c < 4; c++) {
-                    bp.g[k][c] = plane(k, c, b);
-                    bp.gn[k][c] = plane(k, c, b + 1);
+                    cp.g[k][c] = plane(k, c, b);
+                    cp.gn[k][c] = plane(k, c, b + 1);
                 }
-            bp.w = (int)lw_[b];
-            bp.h = (int)lh_[b];
-            bp.tiles_x = (int)tiles_x_[b];
-            bp.mult = b == 0 ? 1.f : 2.f;
-            bp.csf = csf_d_ + (int64_t)b * 128;
-            bp.lum0 = lum0_;
-            bp.span = span_;
-            std::memcpy(bp.blur_w, blur_w_, sizeof(blur_w_));
-            std::memcpy(bp.blur_prefix, blur_prefix_, sizeof(blur_prefix_));
-            std::memcpy(bp.xcm2, xcm2_, sizeof(xcm2_));
-            bp.partials = partials_ + tile_off_[b] * 4;
-            bp.merged = distmap ? merged_ + level_off_[b] : nullptr;
-            bp.merge_div = b == 0 ? 1.f : 2.f;
-            cv_band_kernel<<<(unsigned)tiles_[b], kBandThreads, sizeof(BandSmem), stream_>>>(bp);
+            const int64_t nb = lw_[b] * lh_[b];
+            for (int c = 0; c < 4; c++) {
+                cp.mn[c] = mask_buf_ + c * nb;
+                cp.df[c] = mask_buf_ + (4 + c) * nb;
+                mp.mn[c] = cp.mn[c];
+                mp.df[c] = cp.df[c];
+            }
+            cp.w = mp.w = (int)lw_[b];
+            cp.h = mp.h = (int)lh_[b];
+            cp.tiles_x = (int)ceil_div(lw_[b], kCW);
+            cp.mult = b == 0 ? 1.f : 2.f;
+            cp.csf = csf_d_ + (int64_t)b * 128;
+            cp.lum0 = lum0_;
+            cp.span = span_;
+            const unsigned ctiles = (unsigned)(cp.tiles_x * ceil_div(lh_[b], kCHt));
+            cv_contrast_kernel<<<ctiles, kContrastThreads, 0, stream_>>>(cp);
+            CUDA_CHECK(cudaGetLastError());
+            mp.tiles_x = (int)tiles_x_[b];
+            std::memcpy(mp.blur_w, blur_w_, sizeof(blur_w_));
+            std::memcpy(mp.blur_prefix, blur_prefix_, sizeof(blur_prefix_));
+            std::memcpy(mp.xcm2, xcm2_, sizeof(xcm2_));
+            mp.partials = partials_ + tile_off_[b] * 4;
+            mp.merged = distmap ? merged_ + level_off_[b] : nullptr;
+            mp.merge_div = b == 0 ? 1.f : 2.f;
+            cv_mask_kernel<<<(unsigned)tiles_[b], kBandThreads, sizeof(MaskSmem), stream_>>>(mp);
             CUDA_CHECK(cudaGetLastError());
         }
         timer_.end(t, stream_);
@@ -1240,6 +1303,7 @@ private:
         device_free(up_buf_);
         device_free(ring_);
         device_free(pyr_);
+        device_free(mask_buf_);
         device_free(filt_d_);
         device_free(csf_d_);
         device_free(partials_);
@@ -1247,7 +1311,7 @@ private:
         device_free(merged_);
         device_free(dmap_);
         pinned_free(vals_h_);
-        down_buf_ = up_buf_ = ring_ = pyr_ = filt_d_ = csf_d_ = merged_ = dmap_ = nullptr;
+        down_buf_ = up_buf_ = ring_ = pyr_ = mask_buf_ = filt_d_ = csf_d_ = merged_ = dmap_ = nullptr;
         partials_ = vals_d_ = vals_h_ = nullptr;
         if (last_done_) {
             (void)cudaEventDestroy(last_done_);
@@ -1285,6 +1349,7 @@ private:
     float* up_buf_ = nullptr;
     float* ring_ = nullptr;
     float* pyr_ = nullptr;
+    float* mask_buf_ = nullptr;  // 8 planes of band 0's size: min(|R|,|T|) and |R-T| per channel
     float* filt_d_ = nullptr;
     float* csf_d_ = nullptr;
     double* partials_ = nullptr;
