@@ -1040,6 +1040,23 @@ def run_profile_butter(args):
     log("profile butteraugli: %d pairs x %d calls, norms %s" % (n, args.steps, np.round(norms.cpu().numpy()[0], 4)))
 
 
+def run_profile_cvvdp(args):
+    """Only N 1080p frame pairs through one CVVDP handler (for ncu captures)."""
+    from vship_b200 import abi, api, synth
+    pairs = synth.make_pairs(4, W, H, fmt="yuv420p10", seed=91, unique=4, steps=(4.0, 48.0))
+    cs = abi.yuv420_10bit_bt709(W, H)
+    pinned, host_pairs = pinned_frames(pairs, api)
+    ls = pairs[0][2]
+    h = api.CVVDP(cs, fps=24.0, model="standard_fhd")
+    for f in range(args.profile_cvvdp):
+        a, b = host_pairs[f % len(host_pairs)]
+        score = h.compute(a, b, ls, ls)
+    h.close()
+    for pb in pinned:
+        pb.free()
+    log("profile cvvdp: %d frames, last JOD %.6f" % (args.profile_cvvdp, score))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1066,7 +1083,12 @@ def main():
     ap.add_argument("--profile-uneven", type=int, default=0,
                     help="only run N uneven pairs through the batch graph --steps times and once per "
                          "resolution through handlers (for ncu captures)")
+    ap.add_argument("--profile-cvvdp", type=int, default=0,
+                    help="only run N 1080p frames through one CVVDP handler (for ncu captures)")
     args = ap.parse_args()
+    if args.profile_cvvdp:
+        run_profile_cvvdp(args)
+        return
     if args.profile_pairs:
         run_profile_case(args)
         return

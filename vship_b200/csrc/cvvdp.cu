@@ -111,19 +111,25 @@ struct IngestParams {
 
 // Raw planes straight to the ring (no resize or crop): one 64x64 tile of one clip per CTA,
 // chroma staged in shared memory as in the other metrics' fronts.
-__global__ void __launch_bounds__(256) cv_ingest_kernel(const __grid_constant__ IngestParams p) {
+// kFast selects a compile-time pixel path (colour.cuh) when both clips use it; those paths
+// are BT.709-primaries formats, whose native linear RGB is the BT.709 one they produce.
+template <int kFast>
+__global__ void __launch_bounds__(256, 2) cv_ingest_kernel(const __grid_constant__ IngestParams p) {
     extern __shared__ float stage_mem[];
     const int k = blockIdx.z;
     const ColourParams& cp = p.cp[k];
     const int X0 = blockIdx.x * kStageTile, Y0 = blockIdx.y * kStageTile;
     if (X0 >= cp.W || Y0 >= cp.H) return;
     ChromaStage st{};
-    if (cp.subw || cp.subh) chroma_stage(p.im[k], cp, X0, Y0, stage_mem, st);
+    if (cp.subw || cp.subh) chroma_stage<kFast>(p.im[k], cp, X0, Y0, stage_mem, st);
     float* out = p.slot[k];
     for (int i = threadIdx.x; i < kStageTile * kStageTile; i += blockDim.x) {
         const int X = X0 + (i & (kStageTile - 1)), Y = Y0 + i / kStageTile;
         if (X >= cp.W || Y >= cp.H) continue;
-        const float3 v = encode_pixel(ingest_staged<true>(p.im[k], cp, st, X, Y, X0, Y0), p.disp, p.trc[k], p.prim[k]);
+        float3 lin;
+        if constexpr (kFast == kFastGeneric) lin = ingest_staged<true>(p.im[k], cp, st, X, Y, X0, Y0);
+        else lin = ingest_fast<kFast>(p.im[k], cp, st, X, Y, X0, Y0);
+        const float3 v = encode_pixel(lin, p.disp, p.trc[k], p.prim[k]);
         const int64_t o = (int64_t)Y * cp.W + X;
         out[o] = v.x;
         out[p.n + o] = v.y;
@@ -315,33 +321,46 @@ __device__ __forceinline__ float sensitivity(const float* col, float lum0, float
 // (relative error about 1e-6); 0 for x <= 0.
 __device__ __forceinline__ float pow_pos(float x, float g) { return x > 0.f ? ex2_approx(g * __log2f(x)) : 0.f; }
 
-constexpr int kCW = 64;                   // contrast tile: 64 x 16 pixels of the band
-constexpr int kCHt = 16;
+constexpr int kCW = 64;                   // contrast tile: 64 x 16 pixels of the band, one
+constexpr int kCHt = 16;                  // 2x2 quad per thread
 constexpr int kCoarseW = kCW / 2 + 2;     // 34 coarse columns feed it (expansion taps)
 constexpr int kCoarseH = kCHt / 2 + 2;    // 10 coarse rows
-constexpr int kContrastThreads = 256;
+constexpr int kContrastThreads = (kCW / 2) * (kCHt / 2);  // 256
 
-struct ContrastParams {
+struct ContrastBand {
     const float* g[2][4];   // level b planes (w x h)
     const float* gn[2][4];  // level b+1 planes
-    int w, h, tiles_x;
-    float mult;             // contrast multiplier: 1 at band 0, 2 below
-    const float* csf;       // 4 x 32 log10 sensitivities of this band
-    float lum0, span;       // log10 of the first luminance sample and the axis span
     float* mn[4];           // out: min(|R|, |T|) per channel (w x h)
     float* df[4];           // out: |R - T| per channel
+    const float* csf;       // 4 x 32 log10 sensitivities of this band
+    int w, h, tiles_x, tile_start;
+    float mult;             // contrast multiplier: 1 at band 0, 2 below
+};
+
+// All bands but the baseband in one launch, coarsest first (their few long-running tiles then
+// overlap the finest band's many).
+struct ContrastParams {
+    ContrastBand band[kMaxLevels - 1];
+    int nbands;
+    float lum0, span;       // log10 of the first luminance sample and the axis span
 };
 
 // Laplacian layer of both clips (G_b - expand(G_b+1), the Y channel against the clamped
 // background; lpyr.hpp:177-215), contrast against the background luminance, CSF weighting by
 // the reference clip's background (preGaussianPreCompute_kernel, maskingModel.hpp:5-15).
 // The tile's coarse neighbourhood of all eight next-level planes is staged in shared memory
-// with the expansion's mirror padding already applied.
-__global__ void __launch_bounds__(kContrastThreads) cv_contrast_kernel(const __grid_constant__ ContrastParams p) {
+// with the expansion's mirror padding already applied; each thread expands a 2x2 quad from
+// its 3x3 coarse neighbourhood, separably (even pixels take taps 0.1/0.8/0.1 of the
+// neighbourhood, odd pixels 0.5/0.5 of its last two samples).
+__global__ void __launch_bounds__(kContrastThreads) cv_contrast_kernel(const __grid_constant__ ContrastParams prm) {
     __shared__ float coarse[8][kCoarseH][kCoarseW];
     __shared__ float csf[4][32];
     const int tid = threadIdx.x;
-    const int X0 = (blockIdx.x % p.tiles_x) * kCW, Y0 = (blockIdx.x / p.tiles_x) * kCHt;
+    int bi = 0;
+    while (bi + 1 < prm.nbands && (int)blockIdx.x >= prm.band[bi + 1].tile_start) bi++;
+    const ContrastBand& p = prm.band[bi];
+    const int tile = blockIdx.x - p.tile_start;
+    const int X0 = (tile % p.tiles_x) * kCW, Y0 = (tile / p.tiles_x) * kCHt;
     const int ow = (p.w + 1) / 2, oh = (p.h + 1) / 2;
     const int cx0 = X0 / 2 - 1, cy0 = Y0 / 2 - 1;
     if (tid < 128) csf[tid >> 5][tid & 31] = p.csf[tid];
@@ -357,42 +376,60 @@ __global__ void __launch_bounds__(kContrastThreads) cv_contrast_kernel(const __g
         coarse[q][r][c] = __ldg(p.gn[q >> 2][q & 3] + (int64_t)ry * ow + rx);
     }
     __syncthreads();
-    for (int i = tid; i < kCW * kCHt; i += kContrastThreads) {
-        const int x = X0 + (i % kCW), y = Y0 + i / kCW;
-        if (x >= p.w || y >= p.h) continue;
-        const int px = x & 1, py = y & 1;
-        const int ix0 = (x - X0 - 2 + px) / 2 + 1, iy0 = (y - Y0 - 2 + py) / 2 + 1;  // first taps
-        float e[8];
+    const int qx = tid % (kCW / 2), qy = tid / (kCW / 2);
+    const int x0 = X0 + 2 * qx, y0 = Y0 + 2 * qy;
+    if (x0 >= p.w || y0 >= p.h) return;
+    const float we = 2.f * pyr_k(0), wc = 2.f * pyr_k(2), wo = 2.f * pyr_k(1);  // 0.1, 0.8, 0.5
+    // e[q][v][u]: plane q expanded at pixel (x0 + u, y0 + v)
+    float e[8][2][2];
 #pragma unroll
-        for (int q = 0; q < 8; q++) e[q] = 0.f;
-        for (int ty = 0; ty < 3 - py; ty++) {
-            const float ky = 2.f * pyr_k(2 * ty - 2 + py + 2);
-            for (int tx = 0; tx < 3 - px; tx++) {
-                const float k = (2.f * pyr_k(2 * tx - 2 + px + 2)) * ky;
+    for (int q = 0; q < 8; q++) {
+        float he[3], ho[3];
 #pragma unroll
-                for (int q = 0; q < 8; q++) e[q] = fmaf(k, coarse[q][iy0 + ty][ix0 + tx], e[q]);
+        for (int a = 0; a < 3; a++) {
+            const float c0 = coarse[q][qy + a][qx], c1 = coarse[q][qy + a][qx + 1], c2 = coarse[q][qy + a][qx + 2];
+            he[a] = fmaf(we, c0, fmaf(wc, c1, we * c2));
+            ho[a] = fmaf(wo, c1, wo * c2);
+        }
+        e[q][0][0] = fmaf(we, he[0], fmaf(wc, he[1], we * he[2]));
+        e[q][0][1] = fmaf(we, ho[0], fmaf(wc, ho[1], we * ho[2]));
+        e[q][1][0] = fmaf(wo, he[1], wo * he[2]);
+        e[q][1][1] = fmaf(wo, ho[1], wo * ho[2]);
+    }
+#pragma unroll
+    for (int v = 0; v < 2; v++)
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int x = x0 + u, y = y0 + v;
+            if (x >= p.w || y >= p.h) continue;
+            const int64_t j = (int64_t)y * p.w + x;
+            float con[2][4];
+            float lref = 0.f;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const float lb = fmaxf(e[4 * k][v][u], 0.01f);
+                if (k == 0) lref = lb;
+                const float inv = __frcp_rn(lb);
+                con[k][0] = fminf((__ldg(p.g[k][0] + j) - lb) * inv, 1000.f) * p.mult;
+#pragma unroll
+                for (int c = 1; c < 4; c++)
+                    con[k][c] = fminf((__ldg(p.g[k][c] + j) - e[4 * k + c][v][u]) * inv, 1000.f) * p.mult;
+            }
+            // CSF lookup (computeSensitivityGPU, csf.hpp:60-82) at the reference's background,
+            // the reference's weights (frac on the lower entry); index clamped to the table.
+            float frac = 31.f * (log10f(lref) - prm.lum0) / prm.span;
+            int imin = min(max((int)frac, 0), 31);
+            const int imax = min(31, imin + 1);
+            frac -= (float)imin;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const float logs = csf[c][imin] * frac + csf[c][imax] * (1.f - frac) + kSensitivityCorrection / 20.f;
+                const float s = ex2_approx(logs * 3.32192809488736f) * (c == 1 ? 1.45f : 1.f);
+                const float r = con[0][c] * s, t = con[1][c] * s;
+                p.mn[c][j] = fminf(fabsf(r), fabsf(t));
+                p.df[c][j] = fabsf(r - t);
             }
         }
-        const int64_t j = (int64_t)y * p.w + x;
-        float con[2][4];
-        float lref = 0.f;
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const float lb = fmaxf(e[4 * k], 0.01f);
-            if (k == 0) lref = lb;
-            const float inv = 1.f / lb;
-            con[k][0] = fminf((__ldg(p.g[k][0] + j) - lb) * inv, 1000.f) * p.mult;
-#pragma unroll
-            for (int c = 1; c < 4; c++) con[k][c] = fminf((__ldg(p.g[k][c] + j) - e[4 * k + c]) * inv, 1000.f) * p.mult;
-        }
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const float s = sensitivity(csf[c], p.lum0, p.span, lref) * (c == 1 ? 1.45f : 1.f);
-            const float r = con[0][c] * s, t = con[1][c] * s;
-            p.mn[c][j] = fminf(fabsf(r), fabsf(t));
-            p.df[c][j] = fabsf(r - t);
-        }
-    }
 }
 
 // ---- one Laplacian band: masking and D ---------------------------------------------------
@@ -400,87 +437,138 @@ __global__ void __launch_bounds__(kContrastThreads) cv_contrast_kernel(const __g
 constexpr int kBT = 32;               // output tile
 constexpr int kBH = 8;                // masking blur radius
 constexpr int kBI = kBT + 2 * kBH;    // 48: tile with halo
-constexpr int kBandThreads = 256;
+constexpr int kMaskThreads = 128;
+constexpr int kMaskRPT = 8;           // vertical pass: consecutive output rows per thread
 
-struct MaskParams {
+struct MaskBand {
     const float* mn[4];
     const float* df[4];
-    int w, h, tiles_x;
-    float blur_w[17];
-    float blur_prefix[18];
-    float xcm2[16];         // 2^xcm_weights[k * 4 + c]
-    double* partials;       // 4 sums of D^2 per tile
+    double* partials;       // 4 sums of D^2 per tile of this band
     float* merged;          // distortion-map plane of this band (nullable)
+    int w, h, tiles_x, tile_start;
     float merge_div;
 };
 
-struct MaskSmem {
-    float mn[4][kBI][kBI];     // masking input over the tile and its halo (0 outside the plane)
-    float hb[4][kBI][kBT];     // horizontally blurred
-    float prefix[18];          // cumulative blur weights, for the in-plane renormalisation
-    double red[kBandThreads / 32][4];
+struct MaskParams {
+    MaskBand band[kMaxLevels - 1];  // coarsest first
+    int nbands;
+    float blur_w[17];
+    float xcm2[16];         // 2^xcm_weights[k * 4 + c]
 };
+
+// Channels travel in pairs (0,1) and (2,3) so one 64-bit shared access and one packed FMA
+// serve two of them.
+struct MaskSmem {
+    float2 in[2][kBI][kBI + 1];   // masking input over the tile and its halo (0 outside the plane)
+    float2 hb[2][kBI][kBT + 1];   // horizontally blurred
+    float invx[kBT], invy[kBT];   // 1 / in-plane tap weight of each output column and row
+    double red[kMaskThreads / 32][4];
+};
+
+// Sum of the blur taps that fall inside [0, n) for a window centred on pos (pos clamped into
+// the plane for the tile's padding; their outputs are never used).
+__device__ __forceinline__ float mask_tap_sum(const float* w, int pos, int n) {
+    pos = min(pos, n - 1);
+    float s = 0.f;
+#pragma unroll
+    for (int t = 0; t < 17; t++) {
+        const int q = pos - 8 + t;
+        s += (q >= 0 && q < n) ? w[t] : 0.f;
+    }
+    return s;
+}
 
 // The sigma-3 renormalised blur of min(|R|, |T|) (GaussianSmart_Device, gaussianBlur.hpp:62-119),
 // cross-channel masking, the saturating D with the channel weights (computeD_Kernel,
 // maskingModel.hpp:28-96), the tile's FP64 sums of D^2 and, for the distortion map, the
 // 4-norm over channels (mergeChromaNorm_Kernel, distmap_specifics.hpp:27-33).
-__global__ void __launch_bounds__(kBandThreads) cv_mask_kernel(const __grid_constant__ MaskParams p) {
+__global__ void __launch_bounds__(kMaskThreads) cv_mask_kernel(const __grid_constant__ MaskParams prm) {
     extern __shared__ __align__(16) unsigned char mask_smem_raw[];
     MaskSmem& sm = *reinterpret_cast<MaskSmem*>(mask_smem_raw);
     const int tid = threadIdx.x;
-    const int X0 = (blockIdx.x % p.tiles_x) * kBT, Y0 = (blockIdx.x / p.tiles_x) * kBT;
-    if (tid < 18) sm.prefix[tid] = p.blur_prefix[tid];
-    for (int i = tid; i < 4 * kBI * kBI; i += kBandThreads) {
-        const int c = i / (kBI * kBI), r = (i / kBI) % kBI, x = i % kBI;
-        const int gx = X0 - kBH + x, gy = Y0 - kBH + r;
-        const bool in = gx >= 0 && gx < p.w && gy >= 0 && gy < p.h;
-        sm.mn[c][r][x] = in ? __ldg(p.mn[c] + (int64_t)gy * p.w + gx) : 0.f;
-    }
-    __syncthreads();
-    for (int i = tid; i < 4 * kBI * kBT; i += kBandThreads) {
-        const int c = i / (kBI * kBT);
-        const int r = (i / kBT) % kBI;
-        const int x = i % kBT;
-        const int gx = X0 + x;
-        float v = 0.f;
-        if (gx < p.w) {  // columns past the plane are never read by the vertical pass
-            float s = 0.f;
-#pragma unroll
-            for (int t = 0; t < 17; t++) s = fmaf(sm.mn[c][r][x + t], p.blur_w[t], s);
-            const int beg = max(0, gx - 8) - (gx - 8);   // 0..8
-            const int end = min(p.w, gx + 9) - (gx - 8);  // 9..17
-            v = s / (sm.prefix[end] - sm.prefix[beg]);
+    int bi = 0;
+    while (bi + 1 < prm.nbands && (int)blockIdx.x >= prm.band[bi + 1].tile_start) bi++;
+    const MaskBand& p = prm.band[bi];
+    const int tile = blockIdx.x - p.tile_start;
+    const int X0 = (tile % p.tiles_x) * kBT, Y0 = (tile / p.tiles_x) * kBT;
+    if (tid < kBT) sm.invx[tid] = 1.f / mask_tap_sum(prm.blur_w, X0 + tid, p.w);
+    else if (tid < 2 * kBT) sm.invy[tid - kBT] = 1.f / mask_tap_sum(prm.blur_w, Y0 + tid - kBT, p.h);
+    for (int i = tid; i < kBI * kBI; i += kMaskThreads) {
+        const int r = i / kBI, c = i - r * kBI;
+        const int gx = X0 - kBH + c, gy = Y0 - kBH + r;
+        float2 a = make_float2(0.f, 0.f), b = a;
+        if (gx >= 0 && gx < p.w && gy >= 0 && gy < p.h) {
+            const int64_t j = (int64_t)gy * p.w + gx;
+            a = make_float2(__ldg(p.mn[0] + j), __ldg(p.mn[1] + j));
+            b = make_float2(__ldg(p.mn[2] + j), __ldg(p.mn[3] + j));
         }
-        sm.hb[c][r][x] = v;
+        sm.in[0][r][c] = a;
+        sm.in[1][r][c] = b;
     }
     __syncthreads();
+    // Horizontal pass: 48 rows x 32 columns per channel pair; a work item is four adjacent
+    // output columns of one row, consecutive threads take consecutive rows.
+    for (int u = tid; u < 2 * kBI * (kBT / 4); u += kMaskThreads) {
+        const int pr = u / (kBI * (kBT / 4));
+        const int rem = u - pr * (kBI * (kBT / 4));
+        const int cg = rem / kBI, r = rem - cg * kBI, c0 = cg * 4;
+        float2 v[20];
+#pragma unroll
+        for (int j = 0; j < 20; j++) v[j] = sm.in[pr][r][c0 + j];
+        float2 acc[4];
+#pragma unroll
+        for (int o = 0; o < 4; o++) acc[o] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int t = 0; t < 17; t++) {
+            const float2 wt = make_float2(prm.blur_w[t], prm.blur_w[t]);
+#pragma unroll
+            for (int o = 0; o < 4; o++) acc[o] = __ffma2_rn(wt, v[o + t], acc[o]);
+        }
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+            const float inv = sm.invx[c0 + o];
+            sm.hb[pr][r][c0 + o] = make_float2(acc[o].x * inv, acc[o].y * inv);
+        }
+    }
+    __syncthreads();
+    // Vertical pass: each thread 8 consecutive output rows of one column.
+    const int c = tid & (kBT - 1);
+    const int r0 = (tid >> 5) * kMaskRPT;
+    float2 m[2][kMaskRPT];
+#pragma unroll
+    for (int pr = 0; pr < 2; pr++) {
+        float2 col[kMaskRPT + 16];
+#pragma unroll
+        for (int j = 0; j < kMaskRPT + 16; j++) col[j] = sm.hb[pr][r0 + j][c];
+#pragma unroll
+        for (int o = 0; o < kMaskRPT; o++) {
+            float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int t = 0; t < 17; t++) acc = __ffma2_rn(make_float2(prm.blur_w[t], prm.blur_w[t]), col[o + t], acc);
+            const float inv = sm.invy[r0 + o];
+            m[pr][o] = make_float2(acc.x * inv, acc.y * inv);
+        }
+    }
     const float powmaskc = exp10f(kMaskC);
     const float max_v = exp10f(kDMax);
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int i = tid; i < kBT * kBT; i += kBandThreads) {
-        const int y = i / kBT, x = i % kBT;
-        const int gx = X0 + x, gy = Y0 + y;
+    const int gx = X0 + c;
+#pragma unroll
+    for (int o = 0; o < kMaskRPT; o++) {
+        const int gy = Y0 + r0 + o;
         if (gx >= p.w || gy >= p.h) continue;
-        const int beg = max(0, gy - 8) - (gy - 8);   // 0..8
-        const int end = min(p.h, gy + 9) - (gy - 8);  // 9..17
-        const float inv = 1.f / (sm.prefix[end] - sm.prefix[beg]);
         const int64_t j = (int64_t)gy * p.w + gx;
+        const float mm[4] = {m[0][o].x, m[0][o].y, m[1][o].x, m[1][o].y};
         float cm[4];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            float s = 0.f;
-#pragma unroll
-            for (int t = 0; t < 17; t++) s = fmaf(sm.hb[c][y + t][x], p.blur_w[t], s);
-            cm[c] = pow_pos(powmaskc * fabsf(s * inv), kMaskQ[c]);
-        }
+        for (int k = 0; k < 4; k++) cm[k] = pow_pos(powmaskc * fabsf(mm[k]), kMaskQ[k]);
         float d[4];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const float cmask = fmaf(cm[0], p.xcm2[c], fmaf(cm[1], p.xcm2[4 + c], fmaf(cm[2], p.xcm2[8 + c], cm[3] * p.xcm2[12 + c])));
-            const float du = pow_pos(__ldg(p.df[c] + j), kMaskP) / (1.f + cmask);
-            d[c] = max_v * du / (max_v + du) * (c == 3 ? kChTransW : 1.f);
-            acc[c] += (double)d[c] * (double)d[c];
+        for (int k = 0; k < 4; k++) {
+            const float cmask = fmaf(cm[0], prm.xcm2[k], fmaf(cm[1], prm.xcm2[4 + k], fmaf(cm[2], prm.xcm2[8 + k], cm[3] * prm.xcm2[12 + k])));
+            const float du = __fdividef(pow_pos(__ldg(p.df[k] + j), kMaskP), 1.f + cmask);
+            d[k] = __fdividef(max_v * du, max_v + du) * (k == 3 ? kChTransW : 1.f);
+            acc[k] += (double)(d[k] * d[k]);
         }
         if (p.merged) {
             const float q = (d[0] * d[0]) * (d[0] * d[0]) + (d[1] * d[1]) * (d[1] * d[1]) + (d[2] * d[2]) * (d[2] * d[2]) +
@@ -489,16 +577,16 @@ __global__ void __launch_bounds__(kBandThreads) cv_mask_kernel(const __grid_cons
         }
     }
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        double v = acc[c];
+    for (int k = 0; k < 4; k++) {
+        double v = acc[k];
         for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if ((tid & 31) == 0) sm.red[tid >> 5][c] = v;
+        if ((tid & 31) == 0) sm.red[tid >> 5][k] = v;
     }
     __syncthreads();
     if (tid < 4) {
         double v = 0.0;
-        for (int wi = 0; wi < kBandThreads / 32; wi++) v += sm.red[wi][tid];
-        p.partials[(int64_t)blockIdx.x * 4 + tid] = v;
+        for (int wi = 0; wi < kMaskThreads / 32; wi++) v += sm.red[wi][tid];
+        p.partials[(int64_t)tile * 4 + tid] = v;
     }
 }
 
@@ -1021,7 +1109,7 @@ public:
         const int64_t mn = mw_ * mh_;
         ring_ = device_alloc<float>((size_t)(2 * (int64_t)taps_ * 3 * mn), "temporal ring");
         pyr_ = device_alloc<float>((size_t)(2 * 4 * chan_stride_), "contrast pyramid");
-        if (levels_ > 1) mask_buf_ = device_alloc<float>((size_t)(8 * rw_ * rh_), "band masking planes");
+        if (levels_ > 1) mask_buf_ = device_alloc<float>((size_t)(8 * level_off_[levels_ - 1]), "band masking planes");
         if (mw_ < rw_) up_buf_ = device_alloc<float>((size_t)(2 * 4 * mn + rw_ * mh_), "upscale planes");
         filt_d_ = device_alloc<float>(filt.size(), "temporal filters");
         CUDA_CHECK(cudaMemcpy(filt_d_, filt.data(), filt.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -1111,11 +1199,15 @@ private:
             p.disp = dd_;
             const size_t smem = sizeof(float) * std::max(chroma_stage_floats(cp[0].subw, cp[0].subh),
                                                          chroma_stage_floats(cp[1].subw, cp[1].subh));
-            if (smem > 48 * 1024)
-                CUDA_CHECK(cudaFuncSetAttribute(cv_ingest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const int f0 = fast_path_of(cp[0]);
+            const int fast = f0 == fast_path_of(cp[1]) ? f0 : kFastGeneric;
+            auto kernel = fast == kFastYuv420Bt709 ? cv_ingest_kernel<kFastYuv420Bt709>
+                        : fast == kFastRgb8Srgb    ? cv_ingest_kernel<kFastRgb8Srgb>
+                                                   : cv_ingest_kernel<kFastGeneric>;
+            if (smem > 48 * 1024) CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             const dim3 grid((unsigned)ceil_div(std::max(cp[0].W, cp[1].W), kStageTile),
                             (unsigned)ceil_div(std::max(cp[0].H, cp[1].H), kStageTile), 2);
-            cv_ingest_kernel<<<grid, 256, smem, stream_>>>(p);
+            kernel<<<grid, 256, smem, stream_>>>(p);
             CUDA_CHECK(cudaGetLastError());
         } else {
             EncodeParams p{};
@@ -1212,43 +1304,55 @@ private:
         }
         timer_.end(t, stream_);
 
-        t = timer_.begin(3, "cvvdp_band", stream_);
-        for (int b = 0; b + 1 < levels_; b++) {
+        if (levels_ > 1) {
             ContrastParams cp{};
             MaskParams mp{};
-            for (int k = 0; k < 2; k++)
+            int ctiles = 0, mtiles = 0;
+            cp.nbands = mp.nbands = levels_ - 1;
+            for (int i = 0; i < levels_ - 1; i++) {
+                const int b = levels_ - 2 - i;  // coarsest first
+                ContrastBand& cb = cp.band[i];
+                MaskBand& mb = mp.band[i];
+                const int64_t nb = lw_[b] * lh_[b];
+                for (int k = 0; k < 2; k++)
+                    for (int c = 0; c < 4; c++) {
+                        cb.g[k][c] = plane(k, c, b);
+                        cb.gn[k][c] = plane(k, c, b + 1);
+                    }
+                float* mbuf = mask_buf_ + 8 * level_off_[b];
                 for (int c = 0; c < 4; c++) {
-                    cp.g[k][c] = plane(k, c, b);
-                    cp.gn[k][c] = plane(k, c, b + 1);
+                    cb.mn[c] = mbuf + c * nb;
+                    cb.df[c] = mbuf + (4 + c) * nb;
+                    mb.mn[c] = cb.mn[c];
+                    mb.df[c] = cb.df[c];
                 }
-            const int64_t nb = lw_[b] * lh_[b];
-            for (int c = 0; c < 4; c++) {
-                cp.mn[c] = mask_buf_ + c * nb;
-                cp.df[c] = mask_buf_ + (4 + c) * nb;
-                mp.mn[c] = cp.mn[c];
-                mp.df[c] = cp.df[c];
+                cb.csf = csf_d_ + (int64_t)b * 128;
+                cb.w = mb.w = (int)lw_[b];
+                cb.h = mb.h = (int)lh_[b];
+                cb.tiles_x = (int)ceil_div(lw_[b], kCW);
+                cb.tile_start = ctiles;
+                ctiles += cb.tiles_x * (int)ceil_div(lh_[b], kCHt);
+                cb.mult = b == 0 ? 1.f : 2.f;
+                mb.tiles_x = (int)tiles_x_[b];
+                mb.tile_start = mtiles;
+                mtiles += (int)tiles_[b];
+                mb.partials = partials_ + tile_off_[b] * 4;
+                mb.merged = distmap ? merged_ + level_off_[b] : nullptr;
+                mb.merge_div = b == 0 ? 1.f : 2.f;
             }
-            cp.w = mp.w = (int)lw_[b];
-            cp.h = mp.h = (int)lh_[b];
-            cp.tiles_x = (int)ceil_div(lw_[b], kCW);
-            cp.mult = b == 0 ? 1.f : 2.f;
-            cp.csf = csf_d_ + (int64_t)b * 128;
             cp.lum0 = lum0_;
             cp.span = span_;
-            const unsigned ctiles = (unsigned)(cp.tiles_x * ceil_div(lh_[b], kCHt));
-            cv_contrast_kernel<<<ctiles, kContrastThreads, 0, stream_>>>(cp);
-            CUDA_CHECK(cudaGetLastError());
-            mp.tiles_x = (int)tiles_x_[b];
             std::memcpy(mp.blur_w, blur_w_, sizeof(blur_w_));
-            std::memcpy(mp.blur_prefix, blur_prefix_, sizeof(blur_prefix_));
             std::memcpy(mp.xcm2, xcm2_, sizeof(xcm2_));
-            mp.partials = partials_ + tile_off_[b] * 4;
-            mp.merged = distmap ? merged_ + level_off_[b] : nullptr;
-            mp.merge_div = b == 0 ? 1.f : 2.f;
-            cv_mask_kernel<<<(unsigned)tiles_[b], kBandThreads, sizeof(MaskSmem), stream_>>>(mp);
+            t = timer_.begin(6, "cvvdp_contrast", stream_);
+            cv_contrast_kernel<<<(unsigned)ctiles, kContrastThreads, 0, stream_>>>(cp);
             CUDA_CHECK(cudaGetLastError());
+            timer_.end(t, stream_);
+            t = timer_.begin(7, "cvvdp_mask", stream_);
+            cv_mask_kernel<<<(unsigned)mtiles, kMaskThreads, sizeof(MaskSmem), stream_>>>(mp);
+            CUDA_CHECK(cudaGetLastError());
+            timer_.end(t, stream_);
         }
-        timer_.end(t, stream_);
 
         t = timer_.begin(4, "cvvdp_baseband", stream_);
         const int L = levels_ - 1;
@@ -1349,7 +1453,7 @@ private:
     float* up_buf_ = nullptr;
     float* ring_ = nullptr;
     float* pyr_ = nullptr;
-    float* mask_buf_ = nullptr;  // 8 planes of band 0's size: min(|R|,|T|) and |R-T| per channel
+    float* mask_buf_ = nullptr;  // per band: min(|R|,|T|) and |R-T| of each channel (8 planes)
     float* filt_d_ = nullptr;
     float* csf_d_ = nullptr;
     double* partials_ = nullptr;
