@@ -114,7 +114,7 @@ struct IngestParams {
 // kFast selects a compile-time pixel path (colour.cuh) when both clips use it; those paths
 // are BT.709-primaries formats, whose native linear RGB is the BT.709 one they produce.
 template <int kFast>
-__global__ void __launch_bounds__(256, 2) cv_ingest_kernel(const __grid_constant__ IngestParams p) {
+__global__ void __launch_bounds__(256, 3) cv_ingest_kernel(const __grid_constant__ IngestParams p) {
     extern __shared__ float stage_mem[];
     const int k = blockIdx.z;
     const ColourParams& cp = p.cp[k];
@@ -209,6 +209,7 @@ __global__ void __launch_bounds__(256) cv_temporal_kernel(const __grid_constant_
                 rg = __ldg(reinterpret_cast<const float4*>(f + p.n + i));
                 yv = __ldg(reinterpret_cast<const float4*>(f + 2 * p.n + i));
             } else {
+#pragma unroll 4
                 for (int t = 0; t < p.taps; t++) {
                     const float* f = ring + (int64_t)ring_slot(p, t) * 3 * p.n;
                     const float k0 = __ldg(p.filt + t), k1 = __ldg(p.filt + p.taps + t), k2 = __ldg(p.filt + 2 * p.taps + t),
@@ -364,16 +365,30 @@ __global__ void __launch_bounds__(kContrastThreads) cv_contrast_kernel(const __g
     const int ow = (p.w + 1) / 2, oh = (p.h + 1) / 2;
     const int cx0 = X0 / 2 - 1, cy0 = Y0 / 2 - 1;
     if (tid < 128) csf[tid >> 5][tid & 31] = p.csf[tid];
-    for (int i = tid; i < 8 * kCoarseH * kCoarseW; i += kContrastThreads) {
-        const int q = i / (kCoarseH * kCoarseW), r = (i / kCoarseW) % kCoarseH, c = i % kCoarseW;
-        int rx = cx0 + c, ry = cy0 + r;
-        if (rx < 0) rx = -rx - 1;
-        if (rx >= ow) rx = 2 * ow - rx - 2;
-        if (ry < 0) ry = -ry - 1;
-        if (ry >= oh) ry = 2 * oh - ry - 2;
-        rx = min(max(rx, 0), ow - 1);  // only pixels past the band edge reach beyond the mirror
-        ry = min(max(ry, 0), oh - 1);
-        coarse[q][r][c] = __ldg(p.gn[q >> 2][q & 3] + (int64_t)ry * ow + rx);
+    // Coarse staging: each thread's (up to 11) loads issued before any is stored.
+    constexpr int kStage = 8 * kCoarseH * kCoarseW;
+    constexpr int kPer = (kStage + kContrastThreads - 1) / kContrastThreads;
+    float v[kPer];
+#pragma unroll
+    for (int it = 0; it < kPer; it++) {
+        const int i = tid + it * kContrastThreads;
+        v[it] = 0.f;
+        if (i < kStage) {
+            const int q = i / (kCoarseH * kCoarseW), r = (i / kCoarseW) % kCoarseH, c = i % kCoarseW;
+            int rx = cx0 + c, ry = cy0 + r;
+            if (rx < 0) rx = -rx - 1;
+            if (rx >= ow) rx = 2 * ow - rx - 2;
+            if (ry < 0) ry = -ry - 1;
+            if (ry >= oh) ry = 2 * oh - ry - 2;
+            rx = min(max(rx, 0), ow - 1);  // only pixels past the band edge reach beyond the mirror
+            ry = min(max(ry, 0), oh - 1);
+            v[it] = __ldg(p.gn[q >> 2][q & 3] + (int64_t)ry * ow + rx);
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < kPer; it++) {
+        const int i = tid + it * kContrastThreads;
+        if (i < kStage) (&coarse[0][0][0])[i] = v[it];
     }
     __syncthreads();
     const int qx = tid % (kCW / 2), qy = tid / (kCW / 2);
@@ -491,20 +506,33 @@ __global__ void __launch_bounds__(kMaskThreads) cv_mask_kernel(const __grid_cons
     const MaskBand& p = prm.band[bi];
     const int tile = blockIdx.x - p.tile_start;
     const int X0 = (tile % p.tiles_x) * kBT, Y0 = (tile / p.tiles_x) * kBT;
+    // Halo loads in two batches of 9 elements per thread, every load of a batch issued before
+    // any is stored, so one memory round trip covers nine elements.
+    static_assert(kBI * kBI == 18 * kMaskThreads, "halo splits into 18 elements per thread");
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        float4 v[9];
+#pragma unroll
+        for (int it = 0; it < 9; it++) {
+            const int i = tid + (half * 9 + it) * kMaskThreads;
+            const int r = i / kBI, c = i - r * kBI;
+            const int gx = X0 - kBH + c, gy = Y0 - kBH + r;
+            v[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gx >= 0 && gx < p.w && gy >= 0 && gy < p.h) {
+                const int64_t j = (int64_t)gy * p.w + gx;
+                v[it] = make_float4(__ldg(p.mn[0] + j), __ldg(p.mn[1] + j), __ldg(p.mn[2] + j), __ldg(p.mn[3] + j));
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < 9; it++) {
+            const int i = tid + (half * 9 + it) * kMaskThreads;
+            const int r = i / kBI, c = i - r * kBI;
+            sm.in[0][r][c] = make_float2(v[it].x, v[it].y);
+            sm.in[1][r][c] = make_float2(v[it].z, v[it].w);
+        }
+    }
     if (tid < kBT) sm.invx[tid] = 1.f / mask_tap_sum(prm.blur_w, X0 + tid, p.w);
     else if (tid < 2 * kBT) sm.invy[tid - kBT] = 1.f / mask_tap_sum(prm.blur_w, Y0 + tid - kBT, p.h);
-    for (int i = tid; i < kBI * kBI; i += kMaskThreads) {
-        const int r = i / kBI, c = i - r * kBI;
-        const int gx = X0 - kBH + c, gy = Y0 - kBH + r;
-        float2 a = make_float2(0.f, 0.f), b = a;
-        if (gx >= 0 && gx < p.w && gy >= 0 && gy < p.h) {
-            const int64_t j = (int64_t)gy * p.w + gx;
-            a = make_float2(__ldg(p.mn[0] + j), __ldg(p.mn[1] + j));
-            b = make_float2(__ldg(p.mn[2] + j), __ldg(p.mn[3] + j));
-        }
-        sm.in[0][r][c] = a;
-        sm.in[1][r][c] = b;
-    }
     __syncthreads();
     // Horizontal pass: 48 rows x 32 columns per channel pair; a work item is four adjacent
     // output columns of one row, consecutive threads take consecutive rows.
@@ -534,6 +562,17 @@ __global__ void __launch_bounds__(kMaskThreads) cv_mask_kernel(const __grid_cons
     // Vertical pass: each thread 8 consecutive output rows of one column.
     const int c = tid & (kBT - 1);
     const int r0 = (tid >> 5) * kMaskRPT;
+    const int gx = X0 + c;
+    // |R - T| of this thread's 8 pixels, loaded now so the loads overlap the blur.
+    float dfv[kMaskRPT][4];
+#pragma unroll
+    for (int o = 0; o < kMaskRPT; o++) {
+        const int gy = Y0 + r0 + o;
+        const bool ok = gx < p.w && gy < p.h;
+        const int64_t j = ok ? (int64_t)gy * p.w + gx : 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) dfv[o][k] = ok ? __ldg(p.df[k] + j) : 0.f;
+    }
     float2 m[2][kMaskRPT];
 #pragma unroll
     for (int pr = 0; pr < 2; pr++) {
@@ -552,7 +591,6 @@ __global__ void __launch_bounds__(kMaskThreads) cv_mask_kernel(const __grid_cons
     const float powmaskc = exp10f(kMaskC);
     const float max_v = exp10f(kDMax);
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int gx = X0 + c;
 #pragma unroll
     for (int o = 0; o < kMaskRPT; o++) {
         const int gy = Y0 + r0 + o;
@@ -566,7 +604,7 @@ __global__ void __launch_bounds__(kMaskThreads) cv_mask_kernel(const __grid_cons
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const float cmask = fmaf(cm[0], prm.xcm2[k], fmaf(cm[1], prm.xcm2[4 + k], fmaf(cm[2], prm.xcm2[8 + k], cm[3] * prm.xcm2[12 + k])));
-            const float du = __fdividef(pow_pos(__ldg(p.df[k] + j), kMaskP), 1.f + cmask);
+            const float du = __fdividef(pow_pos(dfv[o][k], kMaskP), 1.f + cmask);
             d[k] = __fdividef(max_v * du, max_v + du) * (k == 3 ? kChTransW : 1.f);
             acc[k] += (double)(d[k] * d[k]);
         }
