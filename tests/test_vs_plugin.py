@@ -10,6 +10,7 @@ The registered names and argument strings are the reference's (src/VshipLib.cpp:
 frame properties are the reference's (src/ssimu2/vapoursynth.hpp, src/butter/vapoursynth.hpp).
 """
 import ctypes
+import json
 import os
 import subprocess
 import threading
@@ -48,7 +49,7 @@ def host(vship_lib, tmp_path_factory):
     L.vsfake_source.restype = vp
     L.vsfake_source.argtypes = [ip, ip, ip, ip, ip, ip, vp]
     L.vsfake_call.restype = vp
-    L.vsfake_call.argtypes = [cp, vp, vp, cp, cp, cp]
+    L.vsfake_call.argtypes = [cp, vp, vp, cp, cp, cp, cp]
     L.vsfake_frame.argtypes = [vp, ip, cp, ctypes.POINTER(ctypes.c_double), vp, cp]
     L.vsfake_free_node.argtypes = [vp]
     from vship_b200 import build
@@ -69,9 +70,10 @@ def source(L, frames, cf=CF_RGB, st=ST_FLOAT, bits=32):
 source.keep = []
 
 
-def call(L, name, ref, dis, ints="", floats=""):
+def call(L, name, ref, dis, ints="", floats="", datas=""):
+    """ints / floats / datas: "key=value" lists separated by ';'."""
     err = ctypes.create_string_buffer(4096)
-    node = L.vsfake_call(name.encode(), ref, dis, ints.encode(), floats.encode(), err)
+    node = L.vsfake_call(name.encode(), ref, dis, ints.encode(), floats.encode(), datas.encode(), err)
     return node, err.value.decode()
 
 
@@ -110,7 +112,8 @@ def test_abi_layout_matches_vapoursynth4_header(tmp_path):
     slots = ["createVideoFilter", "freeNode", "getVideoInfo", "newVideoFrame", "freeFrame", "copyFrame",
              "getFramePropertiesRW", "getStride", "getReadPtr", "getWritePtr", "getFrameWidth", "getFrameHeight",
              "queryVideoFormat", "getFrameFilter", "requestFrameFilter", "setFilterError", "createMap", "freeMap",
-             "mapSetError", "mapGetError", "mapGetInt", "mapSetInt", "mapGetFloat", "mapSetFloat", "mapSetData",
+             "mapSetError", "mapGetError", "mapGetInt", "mapSetInt", "mapGetFloat", "mapSetFloat", "mapGetData",
+             "mapSetData",
              "mapGetNode", "mapConsumeNode", "getPluginByID", "invoke", "getCoreInfo"]
     structs = {
         ("VsAbiVideoFormat", "VSVideoFormat"): ["colorFamily", "sampleType", "bitsPerSample", "bytesPerSample",
@@ -123,7 +126,8 @@ def test_abi_layout_matches_vapoursynth4_header(tmp_path):
     }
     enums = [("vsCfGray", "cfGray"), ("vsCfRGB", "cfRGB"), ("vsCfYUV", "cfYUV"), ("vsStInteger", "stInteger"),
              ("vsStFloat", "stFloat"), ("vsArInitial", "arInitial"), ("vsArAllFramesReady", "arAllFramesReady"),
-             ("vsFmParallel", "fmParallel"), ("vsRpStrictSpatial", "rpStrictSpatial"), ("vsMaReplace", "maReplace"),
+             ("vsFmParallel", "fmParallel"), ("vsFmParallelRequests", "fmParallelRequests"),
+             ("vsRpStrictSpatial", "rpStrictSpatial"), ("vsMaReplace", "maReplace"),
              ("vsPeSuccess", "peSuccess"), ("vsDtUtf8", "dtUtf8"), ("VS_ABI_API_VERSION", "VAPOURSYNTH_API_VERSION"),
              ("VS_ABI_MAKE_VIDEO_ID(vsCfRGB, vsStFloat, 32, 0, 0)", "pfRGBS")]
     lines = ['#include "%s"' % hdr, '#include "%s"' % VS_ABI,
@@ -156,17 +160,18 @@ def test_registration(host):
     assert (pid.value, ns.value, ver.value, apiv.value) == (b"com.lumen.vship", b"vship", (4 << 16) | 1, 4 << 16)
 
 
-def test_cvvdp_reports_not_provided(host):
+@pytest.mark.gpu
+def test_cvvdp_bad_display(gpu, host):
     a = source(host, rgbs_clip(1, 64, 48, 1))
-    node, err = call(host, "CVVDP", a, a)
-    assert node is None and "CVVDP" in err
+    node, err = call(host, "CVVDP", a, a, datas="model_name=no_such_display")
+    assert node is None and "BadDisplayModel" in err, err
 
 
 def test_non_rgbs_without_resize_plugin(host):
     """A YUV clip needs the resize plugin (src/util/torgbs.hpp); the fake core has none."""
     yuv = source(host, np.zeros((1, 3, 48, 64), np.uint8), cf=CF_YUV, st=ST_INT, bits=8)
     rgb = source(host, rgbs_clip(1, 64, 48, 2))
-    for fn in ("SSIMULACRA2", "BUTTERAUGLI"):
+    for fn in ("SSIMULACRA2", "BUTTERAUGLI", "CVVDP"):
         node, err = call(host, fn, yuv, rgb)
         assert node is None and "com.vapoursynth.resize" in err, err
 
@@ -174,7 +179,7 @@ def test_non_rgbs_without_resize_plugin(host):
 def test_differing_clips_rejected(host):
     a = source(host, rgbs_clip(1, 64, 48, 3))
     b = source(host, rgbs_clip(1, 64, 40, 4))
-    for fn in ("SSIMULACRA2", "BUTTERAUGLI"):
+    for fn in ("SSIMULACRA2", "BUTTERAUGLI", "CVVDP"):
         node, err = call(host, fn, a, b)
         assert node is None
         assert api.error_message(4) in err, err
@@ -222,7 +227,7 @@ def test_butteraugli_frames_and_distmap_match_c_abi(gpu, host):
     n, w, h = 2, 256, 160
     ref, dis = rgbs_clip(n, w, h, 20), rgbs_clip(n, w, h, 20)
     dis[:, :, 40:80, 60:120] *= np.float32(0.8)
-    node, err = call(host, "BUTTERAUGLI", source(host, ref), source(host, dis), ints="qnorm=3,distmap=1",
+    node, err = call(host, "BUTTERAUGLI", source(host, ref), source(host, dis), ints="qnorm=3;distmap=1",
                       floats="intensity_multiplier=250")
     assert node is not None, err
     with api.Butteraugli(_rgbs_cs(w, h), qnorm=3, intensity=250.0) as b:
@@ -237,6 +242,44 @@ def test_butteraugli_frames_and_distmap_match_c_abi(gpu, host):
             assert frame(host, node, k, "_BUTTERAUGLI_INFNorm") == norms[2]
             np.testing.assert_array_equal(got, dmap)
     host.vsfake_free_node(node)
+
+
+@pytest.mark.gpu
+def test_cvvdp_frames_match_c_abi(gpu, host, tmp_path):
+    """A CVVDP clip scores its frames in order through one handler: the _CVVDP property of
+    frame n is the JOD of frames 0..n, as the C ABI gives it; distmap=1 returns the map at the
+    display size (resizeToDisplay with a custom display from model_config_json)."""
+    n, w, h = 5, 192, 108
+    ref, dis = rgbs_clip(n, w, h, 30), rgbs_clip(n, w, h, 30)
+    dis += np.float32(0.02) * rgbs_clip(n, w, h, 31)
+    node, err = call(host, "CVVDP", source(host, ref), source(host, dis), datas="model_name=standard_4k")
+    assert node is not None, err
+    got = [frame(host, node, k, "_CVVDP") for k in range(n)]
+    host.vsfake_free_node(node)
+    with api.CVVDP(_rgbs_cs(w, h), fps=24.0, model="standard_4k") as c:
+        want = []
+        for k in range(n):
+            p1, ls = _planes(ref, k)
+            p2, _ = _planes(dis, k)
+            want.append(c.compute(p1, p2, ls))
+    assert got == want
+    assert all(5.0 < v <= 10.0 for v in got), got
+    disp = {"name": "t", "colorspace": "sRGB", "resolution": [96, 54], "viewing_distance_meters": 0.5,
+            "diagonal_size_inches": 10.0, "max_luminance": 250.0, "contrast": 800.0, "E_ambient": 100.0}
+    path = str(tmp_path / "d.json")
+    json.dump({"tiny": disp}, open(path, "w"))
+    node, err = call(host, "CVVDP", source(host, ref), source(host, dis), ints="resizeToDisplay=1;distmap=1",
+                     datas="model_name=tiny;model_config_json=" + path)
+    assert node is not None, err
+    dmap = np.zeros((54, 96), np.float32)
+    v0 = frame(host, node, 0, "_CVVDP", dmap)
+    host.vsfake_free_node(node)
+    with api.CVVDP(_rgbs_cs(w, h), fps=24.0, model="tiny", model_config_json=path, resize_to_display=True) as c:
+        p1, ls = _planes(ref, 0)
+        p2, _ = _planes(dis, 0)
+        s0, m0 = c.compute(p1, p2, ls, distmap=True)
+    assert v0 == s0
+    np.testing.assert_array_equal(dmap, m0)
 
 
 @pytest.mark.gpu

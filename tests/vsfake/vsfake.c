@@ -186,6 +186,13 @@ static int api_map_set_data(VSMap* m, const char* key, const char* d, int size, 
     memcpy(e->data, d, (size_t)size);
     return 0;
 }
+static const char* api_map_get_data(const VSMap* m, const char* key, int idx, int* err) {
+    (void)idx;
+    Entry* e = find(m, key);
+    if (!e || e->type != tData) { if (err) *err = 1; return NULL; }
+    if (err) *err = 0;
+    return e->data;
+}
 static VSNode* api_map_get_node(const VSMap* m, const char* key, int idx, int* err) {
     (void)idx;
     Entry* e = find(m, key);
@@ -272,6 +279,7 @@ int vsfake_load(const char* libpath) {
     g_api.mapGetFloat = api_map_get_float;
     g_api.mapSetFloat = api_map_set_float;
     g_api.mapSetData = api_map_set_data;
+    g_api.mapGetData = api_map_get_data;
     g_api.mapGetNode = api_map_get_node;
     g_api.mapConsumeNode = api_map_consume_node;
     g_api.getPluginByID = api_get_plugin_by_id;
@@ -327,25 +335,27 @@ VSNode* vsfake_source(int w, int h, int nframes, int cf, int st, int bits, const
     return n;
 }
 
-/* Calls registered function `fname` with reference/distorted clips and optional integer and
- * float arguments ("key=value" lists, comma separated); returns the output clip or NULL with
- * the error copied to `err`. */
-VSNode* vsfake_call(const char* fname, VSNode* ref, VSNode* dis, const char* ints, const char* floats, char* err) {
+/* Calls registered function `fname` with reference/distorted clips and optional integer,
+ * float and string arguments ("key=value" lists, separated by ';'); returns the output clip
+ * or NULL with the error copied to `err`. */
+VSNode* vsfake_call(const char* fname, VSNode* ref, VSNode* dis, const char* ints, const char* floats, const char* datas,
+                    char* err) {
     VSMap* in = api_create_map();
     VSMap* out = api_create_map();
     if (ref) api_map_consume_node(in, "reference", ref, 0);
     if (dis) api_map_consume_node(in, "distorted", dis, 0);
-    char buf[512];
-    for (int pass = 0; pass < 2; pass++) {
-        const char* list = pass ? floats : ints;
+    char buf[1024];
+    for (int pass = 0; pass < 3; pass++) {
+        const char* list = pass == 0 ? ints : pass == 1 ? floats : datas;
         if (!list || !*list) continue;
         snprintf(buf, sizeof(buf), "%s", list);
-        for (char* tok = strtok(buf, ","); tok; tok = strtok(NULL, ",")) {
+        for (char* tok = strtok(buf, ";"); tok; tok = strtok(NULL, ";")) {
             char* eq = strchr(tok, '=');
             if (!eq) continue;
             *eq = 0;
-            if (pass) api_map_set_float(in, tok, atof(eq + 1), 0);
-            else api_map_set_int(in, tok, atoll(eq + 1), 0);
+            if (pass == 1) api_map_set_float(in, tok, atof(eq + 1), 0);
+            else if (pass == 0) api_map_set_int(in, tok, atoll(eq + 1), 0);
+            else api_map_set_data(in, tok, eq + 1, (int)strlen(eq + 1), vsDtUtf8, 0);
         }
     }
     VsAbiPublicFunction fn = NULL;

@@ -25,7 +25,7 @@ typedef struct VsAbiApi VsAbiApi;
 enum { vsCfGray = 1, vsCfRGB = 2, vsCfYUV = 3 };
 enum { vsStInteger = 0, vsStFloat = 1 };
 enum { vsArInitial = 0, vsArAllFramesReady = 1 };
-enum { vsFmParallel = 0 };
+enum { vsFmParallel = 0, vsFmParallelRequests = 1 };
 enum { vsRpStrictSpatial = 2 };
 enum { vsMaReplace = 0 };
 enum { vsPeSuccess = 0 };
@@ -129,7 +129,9 @@ struct VsAbiApi {
     double (*mapGetFloat)(const VSMap* map, const char* key, int index, int* error); /* 65 */
     VsAbiSlot slots_66_67[2];
     int (*mapSetFloat)(VSMap* map, const char* key, double d, int append);           /* 68 */
-    VsAbiSlot slots_69_72[4];
+    VsAbiSlot slot_69;
+    const char* (*mapGetData)(const VSMap* map, const char* key, int index, int* error); /* 70 */
+    VsAbiSlot slots_71_72[2];
     int (*mapSetData)(VSMap* map, const char* key, const char* data, int size, int type, int append); /* 73 */
     VSNode* (*mapGetNode)(const VSMap* map, const char* key, int index, int* error); /* 74 */
     VsAbiSlot slot_75;

@@ -4,8 +4,9 @@
 // (src/ssimu2/vapoursynth.hpp, src/butter/vapoursynth.hpp): the same function names, argument
 // strings and defaults, the same conversion of non-RGBS clips through the resize plugin
 // (src/util/torgbs.hpp), the same frame properties and error codes; frames are scored through
-// this library's own C ABI, with a pool of `numStream` handlers shared by VapourSynth's
-// worker threads.  CVVDP is registered but reports that it is not provided, like its C ABI.
+// this library's own C ABI: SSIMULACRA2 and Butteraugli with a pool of `numStream` handlers
+// shared by VapourSynth's worker threads, CVVDP with one handler that keeps the sequence's
+// temporal state (src/cvvdp/vapoursynth.hpp).
 #include <cuda_runtime.h>
 #include <condition_variable>
 #include <cstdint>
@@ -34,6 +35,7 @@ static_assert(offsetof(VsAbiApi, createMap) == 47 * sizeof(void*), "VSAPI slot 4
 static_assert(offsetof(VsAbiApi, mapSetError) == 51 * sizeof(void*), "VSAPI slot 52");
 static_assert(offsetof(VsAbiApi, mapGetInt) == 59 * sizeof(void*), "VSAPI slot 60");
 static_assert(offsetof(VsAbiApi, mapSetFloat) == 67 * sizeof(void*), "VSAPI slot 68");
+static_assert(offsetof(VsAbiApi, mapGetData) == 69 * sizeof(void*), "VSAPI slot 70");
 static_assert(offsetof(VsAbiApi, mapGetNode) == 73 * sizeof(void*), "VSAPI slot 74");
 static_assert(offsetof(VsAbiApi, getPluginByID) == 83 * sizeof(void*), "VSAPI slot 84");
 static_assert(offsetof(VsAbiApi, invoke) == 96 * sizeof(void*), "VSAPI slot 97");
@@ -378,11 +380,119 @@ void butter_create(const VSMap* in, VSMap* out, void*, VSCore* core, const VsAbi
     vsapi->createVideoFilter(out, "vship", &vout, butter_get_frame, butter_free, vsFmParallel, deps, 2, d, core);
 }
 
-// ------------------------------------------------------------------ CVVDP, GpuInfo
+// ------------------------------------------------------------------ CVVDP
 
-void cvvdp_create(const VSMap*, VSMap* out, void*, VSCore*, const VsAbiApi* vsapi) {
-    vsapi->mapSetError(out, Error(Vship_BadErrorType, __FILE__, __LINE__, "CVVDP is not provided by this build").message().c_str());
+// One handler: the metric keeps the sequence's temporal state, so frames are scored one at a
+// time, in request order (src/cvvdp/vapoursynth.hpp:18-99).
+struct CvvdpFilter {
+    VSNode* ref = nullptr;
+    VSNode* dis = nullptr;
+    int distmap = 0;
+    int64_t out_w = 0, out_h = 0;
+    VsAbiVideoFormat gray{};
+    Vship_CVVDPHandler handler{};
+    bool alive = false;
+    std::mutex m;
+};
+
+const VSFrame* cvvdp_get_frame(int n, int reason, void* instance, void**, VSFrameContext* ctx, VSCore* core,
+                               const VsAbiApi* vsapi) {
+    CvvdpFilter* d = static_cast<CvvdpFilter*>(instance);
+    if (reason == vsArInitial) {
+        vsapi->requestFrameFilter(n, d->ref, ctx);
+        vsapi->requestFrameFilter(n, d->dis, ctx);
+        return nullptr;
+    }
+    if (reason != vsArAllFramesReady) return nullptr;
+    const VSFrame* a = vsapi->getFrameFilter(n, d->ref, ctx);
+    const VSFrame* b = vsapi->getFrameFilter(n, d->dis, ctx);
+    VSFrame* dst = d->distmap ? vsapi->newVideoFrame(&d->gray, (int)d->out_w, (int)d->out_h, nullptr, core)
+                              : vsapi->copyFrame(b, core);
+    FramePlanes f = planes_of(a, b, vsapi);
+    double score = 0.0;
+    Vship_Exception rc;
+    std::string msg;
+    {
+        std::lock_guard<std::mutex> g(d->m);
+        rc = d->distmap ? Vship_ComputeCVVDP(d->handler, &score, vsapi->getWritePtr(dst, 0), (int64_t)vsapi->getStride(dst, 0),
+                                             f.p1, f.p2, f.ls1, f.ls2)
+                        : Vship_ComputeCVVDP(d->handler, &score, nullptr, 0, f.p1, f.p2, f.ls1, f.ls2);
+        if (rc != Vship_NoError) {
+            const int len = Vship_CVVDPGetDetailedLastError(d->handler, nullptr, 0);
+            msg.assign((size_t)std::max(len, 1), '\0');
+            Vship_CVVDPGetDetailedLastError(d->handler, &msg[0], len);
+        }
+    }
+    vsapi->freeFrame(a);
+    vsapi->freeFrame(b);
+    if (rc != Vship_NoError) {
+        vsapi->freeFrame(dst);
+        vsapi->setFilterError(msg.c_str(), ctx);
+        return nullptr;
+    }
+    vsapi->mapSetFloat(vsapi->getFramePropertiesRW(dst), "_CVVDP", score, vsMaReplace);
+    return dst;
 }
+
+void cvvdp_free(void* instance, VSCore*, const VsAbiApi* vsapi) {
+    CvvdpFilter* d = static_cast<CvvdpFilter*>(instance);
+    vsapi->freeNode(d->ref);
+    vsapi->freeNode(d->dis);
+    if (d->alive) Vship_CVVDPFree(d->handler);
+    delete d;
+}
+
+std::string get_data(const VSMap* in, const char* key, const char* dflt, const VsAbiApi* vsapi) {
+    int e = 0;
+    const char* v = vsapi->mapGetData(in, key, 0, &e);
+    return e == vsPeSuccess && v ? std::string(v) : std::string(dflt);
+}
+
+void cvvdp_create(const VSMap* in, VSMap* out, void*, VSCore* core, const VsAbiApi* vsapi) {
+    VSNode *ref, *dis;
+    if (!open_pair(in, out, core, vsapi, ref, dis)) return;
+    const int gpu = get_int(in, "gpu_id", 0, vsapi);
+    const int resize = get_int(in, "resizeToDisplay", 0, vsapi);
+    const std::string model = get_data(in, "model_name", "standard_fhd", vsapi);
+    const std::string json = get_data(in, "model_config_json", "", vsapi);
+    if (Vship_GPUFullCheck(gpu) != Vship_NoError) {
+        vsapi->mapSetError(out, global_error().c_str());
+        vsapi->freeNode(ref);
+        vsapi->freeNode(dis);
+        return;
+    }
+    const VsAbiVideoInfo* vi = vsapi->getVideoInfo(ref);
+    float fps = (float)vi->fpsNum / (float)vi->fpsDen;
+    if (!(fps > 0) || fps > 100000.f) fps = 60.f;  // unknown or absurd rates (vapoursynth.hpp:179-183)
+    CvvdpFilter* d = new CvvdpFilter();
+    d->ref = ref;
+    d->dis = dis;
+    d->distmap = get_int(in, "distmap", 0, vsapi);
+    const Vship_Colorspace_t cs = rgbs_colorspace(vi);
+    if (Vship_CVVDPInit3(&d->handler, cs, cs, fps, resize != 0, model.c_str(), json.empty() ? nullptr : json.c_str(),
+                         gpu) != Vship_NoError) {
+        const int len = Vship_CVVDPGetDetailedLastError(d->handler, nullptr, 0);
+        std::string msg((size_t)std::max(len, 1), '\0');
+        Vship_CVVDPGetDetailedLastError(d->handler, &msg[0], len);
+        Vship_CVVDPFree(d->handler);
+        vsapi->mapSetError(out, msg.c_str());
+        cvvdp_free(d, core, vsapi);
+        return;
+    }
+    d->alive = true;
+    Vship_CVVDPGetDistmapResolution(d->handler, &d->out_w, &d->out_h);
+    vsapi->queryVideoFormat(&d->gray, vsCfGray, vsStFloat, 32, 0, 0, core);
+    VsAbiVideoInfo vout = *vi;
+    if (d->distmap) {
+        vout.format = d->gray;
+        vout.width = (int)d->out_w;
+        vout.height = (int)d->out_h;
+    }
+    const VsAbiFilterDependency deps[2] = {{ref, vsRpStrictSpatial}, {dis, vsRpStrictSpatial}};
+    vsapi->createVideoFilter(out, "vship", &vout, cvvdp_get_frame, cvvdp_free, vsFmParallelRequests, deps, 2, d, core);
+}
+
+// ------------------------------------------------------------------ GpuInfo
 
 // Device description (src/VshipLib.cpp:9-59): every device's name without gpu_id, the chosen
 // device's properties with it.
