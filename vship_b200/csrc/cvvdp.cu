@@ -14,9 +14,9 @@
 //                 maskingModel.hpp:5-15)
 //   cv_mask       the sigma-3 masking blur, cross-channel masking, the saturating D and
 //                 per-tile FP64 sums of D^2; one 32x32 tile per CTA (maskingModel.hpp:28-96)
-//   cv_baseband   the baseband: mean luminance, contrast, D and its pooled norm in one CTA
-//                 (lpyr.hpp:219-229, maskingModel.hpp:106-114)
-//   cv_final      pooled norm of every band and channel (pooling.hpp)
+//   cv_pool       pooled norm of every band and channel (pooling.hpp), the last CTA doing the
+//                 baseband: mean luminance, contrast, D (lpyr.hpp:219-229,
+//                 maskingModel.hpp:106-114)
 // The score of the sequence (pooling over bands, channels and frames, JOD) is formed on the
 // host from 4 x bands doubles, as the reference does (main.hpp:135-158, 376-388).
 #include <cuda_runtime.h>
@@ -260,29 +260,67 @@ struct PlaneSet {
 };
 
 // One reduce step of 8 planes (plane blockIdx.y): w x h -> (w+1)/2 x (h+1)/2 with the
-// reference's padding (mirror with edge repeat below 0, without it past the end).
-__global__ void cv_reduce_kernel(const __grid_constant__ PlaneSet p, int w, int h) {
+// reference's padding (mirror with edge repeat below 0, without it past the end).  A CTA makes
+// a 32 x 16 tile of the output: the 68 x 36 input window (mirror resolved while staging) is
+// staged in shared memory, then the separable 5-tap kernel runs along rows and columns.
+constexpr int kRedW = 32, kRedH = 16;
+constexpr int kRedInW = 2 * kRedW + 4, kRedInH = 2 * kRedH + 4;  // 68 x 36
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ int mirror_index(int i, int n) {
+    if (i < 0) i = -i - 1;
+    if (i >= n) i = 2 * n - i - 2;
+    return min(max(i, 0), n - 1);  // only outputs past the plane edge reach beyond the mirror
+}
+
+__global__ void __launch_bounds__(kRedThreads) cv_reduce_kernel(const __grid_constant__ PlaneSet p, int w, int h) {
+    // 72-float rows: even, so a thread's pair of input columns is one aligned float2.
+    constexpr int kStride = kRedInW + 4;
+    __shared__ __align__(16) float in[kRedInH][kStride];
+    __shared__ float hs[kRedInH][kRedW + 1];
     const int nw = (w + 1) / 2, nh = (h + 1) / 2;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nw * nh) return;
-    const int x = i % nw, y = i / nw;
+    const int tiles_x = (nw + kRedW - 1) / kRedW;
+    const int ox0 = (blockIdx.x % tiles_x) * kRedW, oy0 = (blockIdx.x / tiles_x) * kRedH;
     const float* src = p.src[blockIdx.y];
-    float v = 0.f;
+    const int ix0 = 2 * ox0 - 2, iy0 = 2 * oy0 - 2;
+    // Staging: thread (tx, ty) of 64 x 4 loads columns tx and 64 + tx (when < 68) of rows
+    // ty, ty + 4, ...; the mirrored column offsets are formed once.
+    const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;
+    const int ca = mirror_index(ix0 + tx, w);
+    const bool has_b = tx < kRedInW - 64;
+    const int cb = has_b ? mirror_index(ix0 + 64 + tx, w) : 0;
+    constexpr int kRows = kRedInH / 4;  // 9
+    static_assert(kRedInH % 4 == 0, "rows split over 4 thread rows");
+    float va[kRows], vb[kRows];
 #pragma unroll
-    for (int dx = -2; dx <= 2; dx++) {
-        int rx = 2 * x + dx;
-        if (rx < 0) rx = -rx - 1;
-        if (rx >= w) rx = 2 * w - rx - 2;
-        const float kx = pyr_k(dx + 2);
-#pragma unroll
-        for (int dy = -2; dy <= 2; dy++) {
-            int ry = 2 * y + dy;
-            if (ry < 0) ry = -ry - 1;
-            if (ry >= h) ry = 2 * h - ry - 2;
-            v = fmaf(kx * pyr_k(dy + 2), __ldg(src + (int64_t)ry * w + rx), v);
-        }
+    for (int k = 0; k < kRows; k++) {
+        const float* row = src + (int64_t)mirror_index(iy0 + ty + 4 * k, h) * w;
+        va[k] = __ldg(row + ca);
+        vb[k] = has_b ? __ldg(row + cb) : 0.f;
     }
-    p.dst[blockIdx.y][i] = v;
+#pragma unroll
+    for (int k = 0; k < kRows; k++) {
+        in[ty + 4 * k][tx] = va[k];
+        if (has_b) in[ty + 4 * k][64 + tx] = vb[k];
+    }
+    __syncthreads();
+    const float k0 = pyr_k(0), k1 = pyr_k(1), k2 = pyr_k(2);
+    for (int i = threadIdx.x; i < kRedInH * kRedW; i += kRedThreads) {
+        const int r = i / kRedW, x = i - r * kRedW;
+        const float2 a = *reinterpret_cast<const float2*>(&in[r][2 * x]);
+        const float2 b = *reinterpret_cast<const float2*>(&in[r][2 * x + 2]);
+        const float c = in[r][2 * x + 4];
+        hs[r][x] = fmaf(k0, a.x, fmaf(k1, a.y, fmaf(k2, b.x, fmaf(k1, b.y, k0 * c))));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRedH * kRedW; i += kRedThreads) {
+        const int y = i / kRedW, x = i - y * kRedW;
+        const int gx = ox0 + x, gy = oy0 + y;
+        if (gx >= nw || gy >= nh) continue;
+        const float o = fmaf(k0, hs[2 * y][x], fmaf(k1, hs[2 * y + 1][x], fmaf(k2, hs[2 * y + 2][x],
+                             fmaf(k1, hs[2 * y + 3][x], k0 * hs[2 * y + 4][x]))));
+        p.dst[blockIdx.y][(int64_t)gy * nw + gx] = o;
+    }
 }
 
 // Value at (x, y) of a coarse plane expanded to w x h (gaussPyrExpand_Kernel, lpyr.hpp:48-90).
@@ -630,16 +668,23 @@ __global__ void __launch_bounds__(kMaskThreads) cv_mask_kernel(const __grid_cons
 
 // ---- baseband ----------------------------------------------------------------------------
 
-struct BasebandParams {
+struct PoolParams {
+    // bands 0..L-2: tile sums of D^2
+    const double* partials;
+    int64_t tile_off[kMaxLevels];
+    int64_t tiles[kMaxLevels];
+    int64_t pixels[kMaxLevels];
+    int nbands;             // L - 1
+    // baseband (level L-1)
     const float* g[2][4];
     int64_t n;
     const float* csf;
     float lum0, span;
-    double* vals;  // out: 4 pooled norms
-    float* merged; // nullable
+    float* merged;          // nullable
+    double* vals;           // out: 4 pooled norms per band, baseband last
 };
 
-constexpr int kBaseThreads = 1024;
+constexpr int kPoolThreads = 512;
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -651,9 +696,27 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return t;
 }
 
-__global__ void __launch_bounds__(kBaseThreads) cv_baseband_kernel(const __grid_constant__ BasebandParams p) {
-    __shared__ double red[kBaseThreads / 32];
+// Pooled norm sqrt(mean(D^2)) of every band and channel (computeMean<2>, pooling.hpp:54-85):
+// CTA b < L-1 sums band b's tile partials; the last CTA does the baseband: mean background
+// luminance of both clips, contrast, D with the baseband weights (lpyr.hpp:219-229,
+// maskingModel.hpp:106-114) and its norm.
+__global__ void __launch_bounds__(kPoolThreads) cv_pool_kernel(const __grid_constant__ PoolParams p) {
+    __shared__ double red[kPoolThreads / 32];
     __shared__ float sens[4];
+    const int b = blockIdx.x;
+    if (b < p.nbands) {
+        const double* part = p.partials + p.tile_off[b] * 4;
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int64_t t = threadIdx.x; t < p.tiles[b]; t += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < 4; c++) v[c] += part[t * 4 + c];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const double s = block_sum(v[c], red);
+            if (threadIdx.x == 0) p.vals[b * 4 + c] = sqrt(s / (double)p.pixels[b]);
+        }
+        return;
+    }
     double s0 = 0.0, s1 = 0.0;
     for (int64_t i = threadIdx.x; i < p.n; i += blockDim.x) {
         s0 += p.g[0][0][i];
@@ -661,7 +724,8 @@ __global__ void __launch_bounds__(kBaseThreads) cv_baseband_kernel(const __grid_
     }
     const float mean0 = (float)(block_sum(s0, red) / (double)p.n);
     const float mean1 = (float)(block_sum(s1, red) / (double)p.n);
-    if (threadIdx.x < 4) sens[threadIdx.x] = sensitivity(p.csf + 32 * threadIdx.x, p.lum0, p.span, mean0) * kBasebandWeight[threadIdx.x];
+    if (threadIdx.x < 4)
+        sens[threadIdx.x] = sensitivity(p.csf + 32 * threadIdx.x, p.lum0, p.span, mean0) * kBasebandWeight[threadIdx.x];
     __syncthreads();
     const float den0 = fmaxf(0.01f, mean0), den1 = fmaxf(0.01f, mean1);
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -669,8 +733,8 @@ __global__ void __launch_bounds__(kBaseThreads) cv_baseband_kernel(const __grid_
         float d[4];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            const float a = fminf(p.g[0][c][i] / den0, 1000.f), b = fminf(p.g[1][c][i] / den1, 1000.f);
-            d[c] = fabsf(a - b) * sens[c];
+            const float x = fminf(p.g[0][c][i] / den0, 1000.f), y = fminf(p.g[1][c][i] / den1, 1000.f);
+            d[c] = fabsf(x - y) * sens[c];
             acc[c] += (double)d[c] * (double)d[c];
         }
         if (p.merged) {
@@ -682,29 +746,7 @@ __global__ void __launch_bounds__(kBaseThreads) cv_baseband_kernel(const __grid_
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const double t = block_sum(acc[c], red);
-        if (threadIdx.x == 0) p.vals[c] = sqrt(t / (double)p.n);
-    }
-}
-
-// Pooled norm of each band and channel: sqrt(mean(D^2)) from the tile sums (one CTA per band).
-struct FinalParams {
-    const double* partials;
-    int64_t tile_off[kMaxLevels];
-    int64_t tiles[kMaxLevels];
-    int64_t pixels[kMaxLevels];
-    double* vals;
-};
-
-__global__ void __launch_bounds__(256) cv_final_kernel(const __grid_constant__ FinalParams p) {
-    __shared__ double red[8];
-    const int b = blockIdx.x;
-    const double* part = p.partials + p.tile_off[b] * 4;
-    for (int c = 0; c < 4; c++) {
-        double v = 0.0;
-        for (int64_t t = threadIdx.x; t < p.tiles[b]; t += blockDim.x) v += part[t * 4 + c];
-        const double s = block_sum(v, red);
-        if (threadIdx.x == 0) p.vals[b * 4 + c] = sqrt(s / (double)p.pixels[b]);
-        __syncthreads();
+        if (threadIdx.x == 0) p.vals[p.nbands * 4 + c] = sqrt(t / (double)p.n);
     }
 }
 
@@ -1336,8 +1378,8 @@ private:
                 ps.src[q] = plane(q / 4, q % 4, i);
                 ps.dst[q] = plane(q / 4, q % 4, i + 1);
             }
-            const int64_t nn = lw_[i + 1] * lh_[i + 1];
-            cv_reduce_kernel<<<dim3((unsigned)ceil_div(nn, 256), 8), 256, 0, stream_>>>(ps, (int)lw_[i], (int)lh_[i]);
+            const unsigned rtiles = (unsigned)(ceil_div(lw_[i + 1], kRedW) * ceil_div(lh_[i + 1], kRedH));
+            cv_reduce_kernel<<<dim3(rtiles, 8), kRedThreads, 0, stream_>>>(ps, (int)lw_[i], (int)lh_[i]);
             CUDA_CHECK(cudaGetLastError());
         }
         timer_.end(t, stream_);
@@ -1392,31 +1434,26 @@ private:
             timer_.end(t, stream_);
         }
 
-        t = timer_.begin(4, "cvvdp_baseband", stream_);
+        t = timer_.begin(4, "cvvdp_pool", stream_);
         const int L = levels_ - 1;
-        BasebandParams bb{};
-        for (int k = 0; k < 2; k++)
-            for (int c = 0; c < 4; c++) bb.g[k][c] = plane(k, c, L);
-        bb.n = lw_[L] * lh_[L];
-        bb.csf = csf_d_ + (int64_t)L * 128;
-        bb.lum0 = lum0_;
-        bb.span = span_;
-        bb.vals = vals_d_ + 4 * L;
-        bb.merged = distmap ? merged_ + level_off_[L] : nullptr;
-        cv_baseband_kernel<<<1, kBaseThreads, 0, stream_>>>(bb);
-        CUDA_CHECK(cudaGetLastError());
-        if (L > 0) {
-            FinalParams fp{};
-            fp.partials = partials_;
-            for (int b = 0; b < L; b++) {
-                fp.tile_off[b] = tile_off_[b];
-                fp.tiles[b] = tiles_[b];
-                fp.pixels[b] = lw_[b] * lh_[b];
-            }
-            fp.vals = vals_d_;
-            cv_final_kernel<<<L, 256, 0, stream_>>>(fp);
-            CUDA_CHECK(cudaGetLastError());
+        PoolParams pp{};
+        pp.partials = partials_;
+        pp.nbands = L;
+        for (int b = 0; b < L; b++) {
+            pp.tile_off[b] = tile_off_[b];
+            pp.tiles[b] = tiles_[b];
+            pp.pixels[b] = lw_[b] * lh_[b];
         }
+        for (int k = 0; k < 2; k++)
+            for (int c = 0; c < 4; c++) pp.g[k][c] = plane(k, c, L);
+        pp.n = lw_[L] * lh_[L];
+        pp.csf = csf_d_ + (int64_t)L * 128;
+        pp.lum0 = lum0_;
+        pp.span = span_;
+        pp.merged = distmap ? merged_ + level_off_[L] : nullptr;
+        pp.vals = vals_d_;
+        cv_pool_kernel<<<L + 1, kPoolThreads, 0, stream_>>>(pp);
+        CUDA_CHECK(cudaGetLastError());
         timer_.end(t, stream_);
 
         if (distmap) {
