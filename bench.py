@@ -525,6 +525,7 @@ def run_cvvdp(args, rank, local, reference=False):
             h.kernel_timing(False)
             ktimes = {k: round(v[1] / CFRAMES, 4) for k, v in kt.items()}
             sweep["kernels_ms_per_frame"] = ktimes
+            taps = h.geometry()[1]
         for h in handlers:
             h.close()
     for pb in pinned:
@@ -540,6 +541,17 @@ def run_cvvdp(args, rank, local, reference=False):
                     "h2d_bytes_per_step": nthreads * CFRAMES * input_bytes(pairs[:1]),
                     "d2h_bytes_per_step": nthreads * CFRAMES * 8},
             "last_jod": round(last, 6), "clocks": clocks}
+    if not reference and "kernels_ms_per_frame" in sweep:
+        # Dominant HBM-bound kernel: the temporal filter reads the whole ring of both clips
+        # (taps x 3 DKL planes) and writes 4 channel planes per clip.
+        n = W * H
+        algo = 2 * taps * 3 * n * 4 + 2 * 4 * n * 4
+        ms = sweep["kernels_ms_per_frame"]["cvvdp_temporal"]
+        peak, peak_kind = measured_peaks()
+        ach = algo / (ms / 1e3) / 1e9
+        line["roofline"] = {"bound": "hbm", "kernel": "cvvdp_temporal", "achieved": round(ach, 1), "peak": peak,
+                            "peak_source": peak_kind, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                            "algorithmic_bytes_per_launch": algo, "avg_launch_ms": ms, "ring_frames": taps}
     if reference:
         line["impl"] = "reference"
         line["cpu_baseline"] = {"value": round(fps, 2), "unit": "frames/s", "kind": "reference", "cores": nthreads,
