@@ -195,6 +195,10 @@ EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateGradients(VshipExt_SurrogateH
  * fills `out` when max is at least that; -1 on error.  SetModel loads such a vector. */
 EXPORTPREPROCESS int VshipExt_SurrogateModel(VshipExt_SurrogateHandler handler, float* out, int max);
 EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateSetModel(VshipExt_SurrogateHandler handler, const float* model, int count);
+/* Per-kernel CUDA-event timing of a surrogate handler (coarse front, network forward). */
+EXPORTPREPROCESS Vship_Exception VshipExt_SurrogateKernelTiming(VshipExt_SurrogateHandler handler, int enable);
+EXPORTPREPROCESS int VshipExt_SurrogateKernelTimes(VshipExt_SurrogateHandler handler, VshipExt_KernelTime* out, int max,
+                                                   int reset);
 
 /* Metric resolution (after resize and crop) of a handler. */
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2Resolution(Vship_SSIMU2Handler handler, int64_t* width, int64_t* height);

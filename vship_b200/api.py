@@ -117,6 +117,9 @@ def _declare(L):
     L.VshipExt_SurrogateModel.argtypes = [HS, c.c_void_p, c.c_int]
     L.VshipExt_SurrogateModel.restype = c.c_int
     L.VshipExt_SurrogateSetModel.argtypes = [HS, c.c_void_p, c.c_int]
+    L.VshipExt_SurrogateKernelTiming.argtypes = [HS, c.c_int]
+    L.VshipExt_SurrogateKernelTimes.argtypes = [HS, c.c_void_p, c.c_int, c.c_int]
+    L.VshipExt_SurrogateKernelTimes.restype = c.c_int
     L.VshipExt_CVVDPDisplayModel.argtypes = [c.c_char_p, c.c_char_p, c.POINTER(abi.CVVDPDisplay)]
     L.VshipExt_CVVDPGeometry.argtypes = [HC, c.POINTER(c.c_int), c.POINTER(c.c_int)]
     L.VshipExt_CVVDPKernelTiming.argtypes = [HC, c.c_int]
@@ -593,6 +596,16 @@ class Surrogate:
         self._check(self.L.VshipExt_SurrogateTrain(self.h, n, d_inputs, d_targets, epochs, batch, lr, seed,
                                                    hist.ctypes.data))
         return hist
+
+    def kernel_timing(self, enable=True):
+        self._check(self.L.VshipExt_SurrogateKernelTiming(self.h, 1 if enable else 0))
+
+    def kernel_times(self, reset=False):
+        out = (KernelTime * 8)()
+        n = self.L.VshipExt_SurrogateKernelTimes(self.h, out, 8, 1 if reset else 0)
+        if n < 0:
+            check(self.L, abi.BadHandler)
+        return {out[i].name.decode(): (out[i].launches, out[i].total_ms) for i in range(n)}
 
     def gradients(self, n, d_inputs, d_targets):
         import numpy as np

@@ -849,4 +849,15 @@ Vship_Exception VshipExt_SurrogateSetModel(VshipExt_SurrogateHandler handler, co
     });
 }
 
+Vship_Exception VshipExt_SurrogateKernelTiming(VshipExt_SurrogateHandler handler, int enable) {
+    return with_handler(g_surrogate, handler.id, "VshipExt_SurrogateKernelTiming", [&](Slot<SurrogateApi>& s) {
+        require_engine((bool)s.engine);
+        s.engine->timer().enable(enable != 0);
+    });
+}
+
+int VshipExt_SurrogateKernelTimes(VshipExt_SurrogateHandler handler, VshipExt_KernelTime* out, int max, int reset) {
+    return kernel_times(g_surrogate, handler.id, out, max, reset);
+}
+
 }  // extern "C"

@@ -159,53 +159,170 @@ __global__ void sg_pack_against_kernel(const float* __restrict__ coarse, Pyramid
 // Network kernels.  Activations are FP32 [n][c][h][w]; conv weights FP16 [cout][cin][k][k].
 // ------------------------------------------------------------------------------------------
 
-// Forward convolution + bias + ReLU over 16x16 output tiles (grid: tiles, samples).  With
-// kHalfIn the input is the FP16 input block (sample stride `in_stride`), normalised on load
-// as (x - shift[c]) * scale[c]; zero padding outside the level.
-template <int K, int CIN, int COUT, bool kHalfIn>
-__global__ void __launch_bounds__(kConvThreads) sg_conv_fwd(const void* __restrict__ in, int64_t in_stride,
-                                                            const float* __restrict__ norm, const __half* __restrict__ w,
-                                                            const float* __restrict__ b, float* __restrict__ out,
-                                                            int H, int W, int tiles_x) {
-    constexpr int R = K / 2, S = kTileSide + K - 1;
-    __shared__ float s_in[CIN][S][S + 1];
-    __shared__ float s_w[COUT * CIN * K * K];
+// Forward convolution + bias + ReLU (grid: 32 x 8 output tiles, samples).  With kHalfIn the
+// input is the FP16 input block (sample stride `in_stride`), normalised on load as
+// (x - shift[c]) * scale[c]; zero padding outside the level.  Register-blocked: each of the
+// 64 threads makes 4 adjacent pixels of one row for all COUT channels, so one 128-bit shared
+// load of 4 output channels' weights feeds 16 FMAs.  Every output accumulates bias, then
+// input channel, then kernel row, then kernel column, one fmaf each, as a one-pixel loop would.
+constexpr int kFwdTW = 32, kFwdTH = 8, kFwdThreads = (kFwdTW / 4) * kFwdTH;
+
+// With kPool the layer also writes, per tile and channel, the sums of x and x^4 over the
+// tile's pixels (pool[sample][tile][2 * COUT]) for the pooling that follows.
+template <int K, int CIN, int COUT, bool kHalfIn, bool kPool = false>
+__global__ void __launch_bounds__(kFwdThreads) sg_conv_fwd(const void* __restrict__ in, int64_t in_stride,
+                                                           const float* __restrict__ norm, const __half* __restrict__ w,
+                                                           const float* __restrict__ b, float* __restrict__ out,
+                                                           int H, int W, int tiles_x, float* __restrict__ pool = nullptr) {
+    static_assert(COUT % 4 == 0, "weights travel in groups of 4 output channels");
+    constexpr int R = K / 2, SH = kFwdTH + K - 1, SW = kFwdTW + K - 1;
+    constexpr int SP = (SW + 3) / 4 * 4;  // row pitch: 16-byte aligned rows
+    __shared__ __align__(16) float s_in[CIN][SH][SP];
+    __shared__ __align__(16) float s_w[CIN][K][K][COUT];
     const int n = blockIdx.y, tid = threadIdx.x;
-    const int ty0 = (blockIdx.x / tiles_x) * kTileSide, tx0 = (blockIdx.x % tiles_x) * kTileSide;
-    for (int i = tid; i < COUT * CIN * K * K; i += kConvThreads) s_w[i] = __half2float(w[i]);
+    const int ty0 = (blockIdx.x / tiles_x) * kFwdTH, tx0 = (blockIdx.x % tiles_x) * kFwdTW;
+    for (int i = tid; i < COUT * CIN * K * K; i += kFwdThreads) {  // [cout][cin][ky][kx] -> [cin][ky][kx][cout]
+        const int o = i / (CIN * K * K), r = i - o * CIN * K * K;
+        (&s_w[0][0][0][0])[r * COUT + o] = __half2float(w[i]);
+    }
     const int64_t plane = (int64_t)H * W;
-    for (int i = tid; i < CIN * S * S; i += kConvThreads) {
-        const int c = i / (S * S), r = i - c * S * S, yy = r / S, xx = r - yy * S;
-        const int gy = ty0 + yy - R, gx = tx0 + xx - R;
-        float v = 0.f;
-        if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
-            const int64_t o = (int64_t)c * plane + (int64_t)gy * W + gx;
-            if (kHalfIn)
-                v = (__half2float(static_cast<const __half*>(in)[n * in_stride + o]) - norm[c]) * norm[CIN + c];
-            else
-                v = static_cast<const float*>(in)[n * in_stride + o];
+    // Input tile with halo: loads in groups of 16 per thread, all issued before any is stored.
+    constexpr int kElems = CIN * SH * SW, kPer = (kElems + kFwdThreads - 1) / kFwdThreads, kGroup = 16;
+    for (int base = 0; base < kPer; base += kGroup) {
+        float v[kGroup];
+#pragma unroll
+        for (int j = 0; j < kGroup; j++) {
+            const int i = tid + (base + j) * kFwdThreads;
+            v[j] = 0.f;
+            if (base + j < kPer && i < kElems) {
+                const int c = i / (SH * SW), r = i - c * SH * SW, yy = r / SW, xx = r - yy * SW;
+                const int gy = ty0 + yy - R, gx = tx0 + xx - R;
+                if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
+                    const int64_t o = (int64_t)c * plane + (int64_t)gy * W + gx;
+                    if (kHalfIn)
+                        v[j] = (__half2float(static_cast<const __half*>(in)[n * in_stride + o]) - norm[c]) * norm[CIN + c];
+                    else
+                        v[j] = __ldg(static_cast<const float*>(in) + n * in_stride + o);
+                }
+            }
         }
-        s_in[c][yy][xx] = v;
+#pragma unroll
+        for (int j = 0; j < kGroup; j++) {
+            const int i = tid + (base + j) * kFwdThreads;
+            if (base + j < kPer && i < kElems) {
+                const int c = i / (SH * SW), r = i - c * SH * SW, yy = r / SW, xx = r - yy * SW;
+                s_in[c][yy][xx] = v[j];
+            }
+        }
     }
     __syncthreads();
-    const int ly = tid / kTileSide, lx = tid % kTileSide;
-    const int gy = ty0 + ly, gx = tx0 + lx;
-    if (gy >= H || gx >= W) return;
-    float acc[COUT];
+    const int ly = tid / (kFwdTW / 4), lx0 = (tid % (kFwdTW / 4)) * 4;
+    const int gy = ty0 + ly, gx0 = tx0 + lx0;
+    if (!kPool && (gy >= H || gx0 >= W)) return;  // with kPool every thread reaches the reduction
+    float acc[4][COUT];
 #pragma unroll
-    for (int o = 0; o < COUT; o++) acc[o] = b[o];
+    for (int o = 0; o < COUT; o++) {
+        const float bo = b[o];
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[q][o] = bo;
+    }
     for (int c = 0; c < CIN; c++)
 #pragma unroll
-        for (int ky = 0; ky < K; ky++)
+        for (int ky = 0; ky < K; ky++) {
+            float v[4 + K - 1];
+            const float4 v4 = *reinterpret_cast<const float4*>(&s_in[c][ly + ky][lx0]);
+            v[0] = v4.x; v[1] = v4.y; v[2] = v4.z; v[3] = v4.w;
 #pragma unroll
-            for (int kx = 0; kx < K; kx++) {
-                const float v = s_in[c][ly + ky][lx + kx];
+            for (int e = 4; e < 4 + K - 1; e++) v[e] = s_in[c][ly + ky][lx0 + e];
 #pragma unroll
-                for (int o = 0; o < COUT; o++) acc[o] = fmaf(s_w[(o * CIN + c) * K * K + ky * K + kx], v, acc[o]);
+            for (int kx = 0; kx < K; kx++)
+#pragma unroll
+                for (int o4 = 0; o4 < COUT / 4; o4++) {
+                    const float4 wv = *reinterpret_cast<const float4*>(&s_w[c][ky][kx][4 * o4]);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        acc[q][4 * o4 + 0] = fmaf(wv.x, v[q + kx], acc[q][4 * o4 + 0]);
+                        acc[q][4 * o4 + 1] = fmaf(wv.y, v[q + kx], acc[q][4 * o4 + 1]);
+                        acc[q][4 * o4 + 2] = fmaf(wv.z, v[q + kx], acc[q][4 * o4 + 2]);
+                        acc[q][4 * o4 + 3] = fmaf(wv.w, v[q + kx], acc[q][4 * o4 + 3]);
+                    }
+                }
+        }
+    const bool row_ok = gy < H;
+    float* dst = out + (int64_t)n * COUT * plane + (int64_t)gy * W + gx0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (!row_ok || gx0 + q >= W) break;
+#pragma unroll
+        for (int o = 0; o < COUT; o++) dst[o * plane + q] = fmaxf(acc[q][o], 0.f);
+    }
+    if constexpr (kPool) {
+        __shared__ float red[kFwdThreads / 32][2 * COUT];
+        float s1[COUT], s4[COUT];
+#pragma unroll
+        for (int o = 0; o < COUT; o++) {
+            s1[o] = s4[o] = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float x = (row_ok && gx0 + q < W) ? fmaxf(acc[q][o], 0.f) : 0.f, x2 = x * x;
+                s1[o] += x;
+                s4[o] = fmaf(x2, x2, s4[o]);
             }
-    float* dst = out + (int64_t)n * COUT * plane + (int64_t)gy * W + gx;
 #pragma unroll
-    for (int o = 0; o < COUT; o++) dst[o * plane] = fmaxf(acc[o], 0.f);
+            for (int off = 16; off > 0; off >>= 1) {
+                s1[o] += __shfl_xor_sync(0xffffffffu, s1[o], off);
+                s4[o] += __shfl_xor_sync(0xffffffffu, s4[o], off);
+            }
+        }
+        if ((tid & 31) == 0)
+#pragma unroll
+            for (int o = 0; o < COUT; o++) {
+                red[tid >> 5][o] = s1[o];
+                red[tid >> 5][COUT + o] = s4[o];
+            }
+        __syncthreads();
+        if (tid < 2 * COUT) {
+            float v = 0.f;
+#pragma unroll
+            for (int wi = 0; wi < kFwdThreads / 32; wi++) v += red[wi][tid];
+            pool[((int64_t)n * gridDim.x + blockIdx.x) * 2 * COUT + tid] = v;
+        }
+    }
+}
+
+// Per sample: mean and 4-norm of each conv3 channel over the level from the tile sums of the
+// last layer (fixed order: deterministic); also keeps mean(x^4) for the backward pass.
+__global__ void __launch_bounds__(256) sg_pool_finish(const float* __restrict__ pool, int tiles, int HW,
+                                                      float* __restrict__ feat, float* __restrict__ m4, int level) {
+    __shared__ float red[8][2 * kC3];
+    const int n = blockIdx.x, tid = threadIdx.x;
+    const float* part = pool + (int64_t)n * tiles * 2 * kC3;
+    float v[2 * kC3];
+#pragma unroll
+    for (int k = 0; k < 2 * kC3; k++) v[k] = 0.f;
+    for (int t = tid; t < tiles; t += 256)
+#pragma unroll
+        for (int k = 0; k < 2 * kC3; k++) v[k] += part[t * 2 * kC3 + k];
+#pragma unroll
+    for (int k = 0; k < 2 * kC3; k++)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], off);
+    if ((tid & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 2 * kC3; k++) red[tid >> 5][k] = v[k];
+    __syncthreads();
+    if (tid < 2 * kC3) {
+        float t = 0.f;
+        for (int wi = 0; wi < 8; wi++) t += red[wi][tid];
+        t /= (float)HW;
+        const int c = tid % kC3;
+        if (tid < kC3) {
+            feat[n * kFeat + level * 2 * kC3 + c] = t;
+        } else {
+            m4[n * 2 * kC3 + level * kC3 + c] = t;
+            feat[n * kFeat + level * 2 * kC3 + kC3 + c] = sqrtf(sqrtf(t + kPoolEps));
+        }
+    }
 }
 
 // Gradient of the input of a conv + ReLU layer: din[c][y][x] = sum over o, taps of
@@ -319,52 +436,6 @@ __global__ void __launch_bounds__(kConvThreads) sg_conv_bwd_weight(const void* _
 #pragma unroll
         for (int k = 0; k < K * K; k++) atomicAdd(dW + (o * CIN + c) * K * K + k, acc[k]);
         if (c == 0) atomicAdd(db + o, accb);
-    }
-}
-
-// Per sample: mean and 4-norm of each conv3 channel over the level (FP32 partials, block
-// reduction); also keeps mean(x^4) for the backward pass.
-__global__ void __launch_bounds__(256) sg_pool_fwd(const float* __restrict__ act, int HW, float* __restrict__ feat,
-                                                   float* __restrict__ m4, int level) {
-    __shared__ float red[8][2 * kC3];
-    const int n = blockIdx.x, tid = threadIdx.x;
-    float s1[kC3], s4[kC3];
-#pragma unroll
-    for (int c = 0; c < kC3; c++) s1[c] = s4[c] = 0.f;
-    const float* base = act + (int64_t)n * kC3 * HW;
-    for (int i = tid; i < HW; i += 256) {
-#pragma unroll
-        for (int c = 0; c < kC3; c++) {
-            const float x = base[(int64_t)c * HW + i], x2 = x * x;
-            s1[c] += x;
-            s4[c] = fmaf(x2, x2, s4[c]);
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < kC3; c++)
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            s1[c] += __shfl_xor_sync(0xffffffffu, s1[c], off);
-            s4[c] += __shfl_xor_sync(0xffffffffu, s4[c], off);
-        }
-    if ((tid & 31) == 0)
-#pragma unroll
-        for (int c = 0; c < kC3; c++) {
-            red[tid >> 5][c] = s1[c];
-            red[tid >> 5][kC3 + c] = s4[c];
-        }
-    __syncthreads();
-    if (tid < 2 * kC3) {
-        float v = 0.f;
-        for (int wi = 0; wi < 8; wi++) v += red[wi][tid];
-        v /= (float)HW;
-        const int c = tid % kC3;
-        if (tid < kC3) {
-            feat[n * kFeat + level * 2 * kC3 + c] = v;
-        } else {
-            m4[n * 2 * kC3 + level * kC3 + c] = v;
-            feat[n * kFeat + level * 2 * kC3 + kC3 + c] = sqrtf(sqrtf(v + kPoolEps));
-        }
     }
 }
 
@@ -817,6 +888,9 @@ private:
         feat_ = device_alloc<float>(cap * kFeat, "surrogate features");
         dfeat_ = device_alloc<float>(cap * kFeat, "surrogate feature gradients");
         m4_ = device_alloc<float>(cap * 2 * kC3, "surrogate pooling moments");
+        const int64_t tiles = std::max(ceil_div(l3_.w, kFwdTW) * ceil_div(l3_.h, kFwdTH),
+                                       ceil_div(l4_.w, kFwdTW) * ceil_div(l4_.h, kFwdTH));
+        pool_ = device_alloc<float>(cap * (size_t)tiles * 2 * kC3, "surrogate pooling partials");
         loss_acc_ = device_alloc<float>(2, "surrogate loss");
         batch_cap_ = kBatchCap;
     }
@@ -829,18 +903,18 @@ private:
     void forward(int n, const __half* in, cudaStream_t st) {
         for (int L = 0; L < 2; L++) {
             const Level& lv = L ? l4_ : l3_;
-            const int H = lv.h, W = lv.w, tx = (int)ceil_div(W, kTileSide);
-            const dim3 grid((unsigned)tiles_of(H, W), (unsigned)n);
+            const int H = lv.h, W = lv.w, tx = (int)ceil_div(W, kFwdTW);
+            const dim3 grid((unsigned)(tx * ceil_div(H, kFwdTH)), (unsigned)n);
             float* a1 = act1_ + level_base(L, n, kC1);
             float* a2 = act2_ + level_base(L, n, kC2);
             float* a3 = act3_ + level_base(L, n, kC3);
-            sg_conv_fwd<3, kCin, kC1, true><<<grid, kConvThreads, 0, st>>>(in + lv.off, block_, norm_, params16_ + oW1,
-                                                                        params_ + ob1, a1, H, W, tx);
-            sg_conv_fwd<3, kC1, kC2, false><<<grid, kConvThreads, 0, st>>>(a1, (int64_t)kC1 * H * W, nullptr,
-                                                                         params16_ + oW2, params_ + ob2, a2, H, W, tx);
-            sg_conv_fwd<1, kC2, kC3, false><<<grid, kConvThreads, 0, st>>>(a2, (int64_t)kC2 * H * W, nullptr,
-                                                                         params16_ + oW3, params_ + ob3, a3, H, W, tx);
-            sg_pool_fwd<<<(unsigned)n, 256, 0, st>>>(a3, H * W, feat_, m4_, L);
+            sg_conv_fwd<3, kCin, kC1, true><<<grid, kFwdThreads, 0, st>>>(in + lv.off, block_, norm_, params16_ + oW1,
+                                                                       params_ + ob1, a1, H, W, tx);
+            sg_conv_fwd<3, kC1, kC2, false><<<grid, kFwdThreads, 0, st>>>(a1, (int64_t)kC1 * H * W, nullptr,
+                                                                        params16_ + oW2, params_ + ob2, a2, H, W, tx);
+            sg_conv_fwd<1, kC2, kC3, false, true><<<grid, kFwdThreads, 0, st>>>(
+                a2, (int64_t)kC2 * H * W, nullptr, params16_ + oW3, params_ + ob3, a3, H, W, tx, pool_);
+            sg_pool_finish<<<(unsigned)n, 256, 0, st>>>(pool_, (int)grid.x, H * W, feat_, m4_, L);
             CUDA_CHECK(cudaGetLastError());
         }
     }
@@ -878,7 +952,7 @@ private:
     }
 
     void free_batch() {
-        for (float** p : {&act1_, &act2_, &act3_, &d1_, &d2_, &d3_, &feat_, &dfeat_, &m4_, &loss_acc_}) {
+        for (float** p : {&act1_, &act2_, &act3_, &d1_, &d2_, &d3_, &feat_, &dfeat_, &m4_, &pool_, &loss_acc_}) {
             device_free(*p);
             *p = nullptr;
         }
@@ -921,6 +995,7 @@ private:
     std::vector<float> host_params_, host_norm_;
     int batch_cap_ = 0;
     float *act1_ = nullptr, *act2_ = nullptr, *act3_ = nullptr;
+    float* pool_ = nullptr;  // per-tile channel sums of the last layer
     float *d1_ = nullptr, *d2_ = nullptr, *d3_ = nullptr;
     float *feat_ = nullptr, *dfeat_ = nullptr, *m4_ = nullptr, *loss_acc_ = nullptr;
     KernelTimer timer_;
