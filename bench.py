@@ -425,26 +425,17 @@ def run_butteraugli(args, world, rank, local):
     ktimes = h.kernel_times(reset=True)
     h.kernel_timing(False)
     per_pair_ms = {k: round(v[1] / BBATCH, 4) for k, v in ktimes.items()}
-    pinned, host_pairs = pinned_frames(pairs, api)
-    out = np.zeros((BH, BW), np.float32)
-    h.compute(host_pairs[0][0], host_pairs[0][1], ls, ls)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for i in range(BBATCH):
-            res, _ = h.compute(host_pairs[i][0], host_pairs[i][1], ls, ls, distmap=True)
-    e2e_s = time.perf_counter() - t0
     h.close()
-    for pb in pinned:
-        pb.free()
+    e2e, e2e_threads, sweep = butter_e2e(args, pairs, cs, ls, local)
     peak, peak_kind = measured_peaks()
     achieved = B_ALGO_BYTES / (sum(v[1] for v in ktimes.values()) / BBATCH / 1e3) / 1e9
     line = {"metric": BMETRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": BWORKLOAD, "pairs_per_step": BBATCH, "width": BW, "height": BH},
-            "e2e": {"value": round(BBATCH * args.steps / e2e_s, 2), "unit": UNIT,
-                    "api": "Vship_ComputeButteraugli with distortion map, one thread",
+            "e2e": {"value": round(e2e, 2), "unit": UNIT,
+                    "api": "Vship_ComputeButteraugli with distortion map, pinned frames",
+                    "threads_handlers": e2e_threads, "threads_swept": sweep,
                     "h2d_bytes_per_step": BBATCH * 2 * 3 * BW * BH, "d2h_bytes_per_step": BBATCH * (BW * BH * 4 + 24)},
             "kernels_ms_per_pair": per_pair_ms,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": peak_kind,
@@ -558,6 +549,73 @@ def run_cvvdp(args, rank, local, reference=False):
                                 "sample": "the reference has no CPU implementation: its own CUDA build on the B200"}
         line["e2e"]["h2d_bytes_per_step"] = 0
         line["e2e"]["d2h_bytes_per_step"] = 0
+    print(json.dumps(line), flush=True)
+
+
+def butter_e2e(args, pairs, cs, ls, local, lib=None):
+    """Butteraugli end to end through Vship_ComputeButteraugli (distortion map returned) with
+    pinned host frames: T host threads, each with its own handler, best of T in 1, 2, 4, 8.
+    Returns (pairs/s, T, sweep)."""
+    import threading
+    import torch
+    from vship_b200 import api
+    pinned, host_pairs = pinned_frames(pairs, api, lib=lib)
+    sweep, best = {}, None
+    for nthreads in (1, 2, 4, 8):
+        handlers = [api.Butteraugli(cs, qnorm=5, intensity=203.0, gpu_id=local, lib=lib) for _ in range(nthreads)]
+
+        def worker(k, reps):
+            for _ in range(reps):
+                for i in range(k, len(host_pairs), nthreads):
+                    handlers[k].compute(host_pairs[i][0], host_pairs[i][1], ls, ls, distmap=True)
+
+        def run(reps):
+            th = [threading.Thread(target=worker, args=(k, reps)) for k in range(nthreads)]
+            for x in th:
+                x.start()
+            for x in th:
+                x.join()
+
+        run(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run(args.steps)
+        dt = time.perf_counter() - t0
+        v = len(host_pairs) * args.steps / dt
+        sweep[nthreads] = round(v, 2)
+        if best is None or v > best[0]:
+            best = (v, nthreads)
+        for h in handlers:
+            h.close()
+    for pb in pinned:
+        pb.free()
+    return best[0], best[1], sweep
+
+
+def run_butteraugli_reference(args, rank, local):
+    """Reference arm of the Butteraugli line: the reference library built from its own sources
+    (oracle/_ref) on the same 4K pairs, end to end through its C API."""
+    import torch
+    from vship_b200 import abi, api, synth
+    torch.cuda.set_device(local)
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libvship_ref.so")
+    if not os.path.exists(ref_path):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/build_ref.sh)"}))
+        return
+    L = api.load_library(ref_path)
+    pairs = synth.make_pairs(BBATCH, BW, BH, fmt="rgb8", seed=77 + rank, unique=4, blur=(0.0, 1.5))
+    cs = abi.srgb8(BW, BH)
+    v, nthreads, sweep = butter_e2e(args, pairs, cs, pairs[0][2], local, lib=L)
+    line = {"impl": "reference", "metric": BMETRIC, "value": round(v, 2), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": BWORKLOAD, "pairs_per_step": BBATCH, "width": BW, "height": BH,
+                       "library": "Vship 4.1.0 built from its sources with nvcc for sm_100a (oracle/build_ref.sh)",
+                       "api": "Vship_ComputeButteraugli with distortion map, pinned frames",
+                       "threads_handlers": nthreads, "threads_swept": sweep},
+            "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "kind": "reference", "cores": nthreads,
+                             "sample": "the reference has no CPU implementation: its own CUDA build on the B200"}}
     print(json.dumps(line), flush=True)
 
 
@@ -1114,8 +1172,11 @@ def main():
         args.warmup = 3
     world, rank, local = dist_env()
     if args.metric == "butteraugli":
-        if args.impl == "ours" and rank == 0:
-            run_butteraugli(args, world, rank, local)
+        if rank == 0:
+            if args.impl == "ours":
+                run_butteraugli(args, world, rank, local)
+            else:
+                run_butteraugli_reference(args, rank, local)
         return
     if args.metric == "cvvdp":
         if rank == 0:
