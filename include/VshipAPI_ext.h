@@ -134,6 +134,13 @@ EXPORTPREPROCESS Vship_Exception VshipExt_ComputeSSIMU2Batch(VshipExt_SSIMU2Batc
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchSetTileRows(VshipExt_SSIMU2BatchHandler handler, int rows);
 /* Rows used by the last batch (0 before the first). */
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchTileRows(VshipExt_SSIMU2BatchHandler handler, int* rows);
+/* Test hook for the launch's bounded dependency waits: the next launch of this handler runs
+ * its front grid without its last tile, so the map tiles of that pair wait for a pyramid that
+ * is never finished.  The wait gives up after its 2 s limit and sets the launch's error word;
+ * VshipExt_ComputeSSIMU2Batch then fails with Vship_HIPError (VshipExt_ComputeSSIMU2BatchDevice
+ * reports it on the next call), and the launches after it are whole again.  Nothing faults
+ * and the context stays usable. */
+EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchTestHoldFrontTile(VshipExt_SSIMU2BatchHandler handler);
 EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2BatchKernelTiming(VshipExt_SSIMU2BatchHandler handler, int enable);
 EXPORTPREPROCESS int VshipExt_SSIMU2BatchKernelTimes(VshipExt_SSIMU2BatchHandler handler, VshipExt_KernelTime* out,
                                                      int max, int reset);

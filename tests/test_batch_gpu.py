@@ -203,6 +203,40 @@ def test_batch_errors(gpu, mix):
     assert L.VshipExt_SSIMU2BatchFree(abi.SSIMU2BatchHandler(12345)) == abi.BadHandler
 
 
+def test_batch_wait_limit_reports_error_and_recovers(gpu, mix):
+    """A launch whose last front tile is held back: the map tiles of that pair wait for a
+    pyramid that is never finished, the bounded wait gives up after its 2 s limit and sets the
+    launch's error word, and the call reports Vship_HIPError.  The wait ends, nothing faults,
+    and the next launches give the scores of launches without the hold, through both entries."""
+    import time
+    import torch
+    items = [(m["cs"], m["cs"], m["p1"], m["p2"], m["ls"], m["ls"]) for m in mix[:5]]
+    with api.SSIMU2Batch() as b:
+        b.set_tile_rows(32)
+        want = b.compute(items)
+        b.hold_front_tile()
+        t0 = time.perf_counter()
+        with pytest.raises(api.VshipError) as e:
+            b.compute(items)
+        waited = time.perf_counter() - t0
+        assert e.value.code == abi.HIPError
+        assert "time limit" in str(e.value)
+        assert 1.9 < waited < 30.0, waited
+        np.testing.assert_array_equal(b.compute(items), want)
+        # device entry: the launch is queued without waiting, so the next call reports it
+        dev = _device_items(mix[:5])
+        s = torch.zeros(len(dev), dtype=torch.float64, device="cuda")
+        b.hold_front_tile()
+        b.compute_device(dev, s.data_ptr())
+        torch.cuda.synchronize()
+        with pytest.raises(api.VshipError) as e:
+            b.compute_device(dev, s.data_ptr())
+        assert e.value.code == abi.HIPError
+        b.compute_device(dev, s.data_ptr())
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(s.cpu().numpy(), want)
+
+
 def test_batch_uneven_1080p_and_4k(gpu):
     """Large frames of the uneven workload: batch scores equal the per-pair handler path."""
     import torch

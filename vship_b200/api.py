@@ -95,6 +95,7 @@ def _declare(L):
     L.VshipExt_ComputeSSIMU2Batch.argtypes = [HBt, c.c_int, FPp, c.POINTER(c.c_double), c.c_void_p]
     L.VshipExt_SSIMU2BatchSetTileRows.argtypes = [HBt, c.c_int]
     L.VshipExt_SSIMU2BatchTileRows.argtypes = [HBt, c.POINTER(c.c_int)]
+    L.VshipExt_SSIMU2BatchTestHoldFrontTile.argtypes = [HBt]
     L.VshipExt_SSIMU2BatchKernelTiming.argtypes = [HBt, c.c_int]
     L.VshipExt_SSIMU2BatchKernelTimes.argtypes = [HBt, c.c_void_p, c.c_int, c.c_int]
     L.VshipExt_SSIMU2BatchKernelTimes.restype = c.c_int
@@ -508,6 +509,11 @@ class SSIMU2Batch:
         r = ctypes.c_int(0)
         self._check(self.L.VshipExt_SSIMU2BatchTileRows(self.h, ctypes.byref(r)))
         return r.value
+
+    def hold_front_tile(self):
+        """Test hook: the next launch leaves its last front tile out, so that its bounded
+        dependency wait runs out and the call reports Vship_HIPError."""
+        self._check(self.L.VshipExt_SSIMU2BatchTestHoldFrontTile(self.h))
 
     def kernel_timing(self, enable=True):
         self._check(self.L.VshipExt_SSIMU2BatchKernelTiming(self.h, 1 if enable else 0))

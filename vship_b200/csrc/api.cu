@@ -707,6 +707,13 @@ Vship_Exception VshipExt_SSIMU2BatchTileRows(VshipExt_SSIMU2BatchHandler handler
     });
 }
 
+Vship_Exception VshipExt_SSIMU2BatchTestHoldFrontTile(VshipExt_SSIMU2BatchHandler handler) {
+    return with_handler(g_batch, handler.id, "VshipExt_SSIMU2BatchTestHoldFrontTile", [&](Slot<Ssimu2BatchApi>& s) {
+        require_engine((bool)s.engine);
+        s.engine->hold_front_tile();
+    });
+}
+
 Vship_Exception VshipExt_SSIMU2BatchKernelTiming(VshipExt_SSIMU2BatchHandler handler, int enable) {
     return with_handler(g_batch, handler.id, "VshipExt_SSIMU2BatchKernelTiming", [&](Slot<Ssimu2BatchApi>& s) {
         require_engine((bool)s.engine);

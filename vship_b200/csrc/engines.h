@@ -57,6 +57,8 @@ struct Ssimu2BatchApi {
     virtual void compute(int n, const VshipExt_FramePair* pairs, double* scores, float* features) = 0;
     virtual void set_tile_rows(int rows) = 0;
     virtual int tile_rows() const = 0;
+    // Test hook: the next launch leaves its last front tile unlaunched (one launch only).
+    virtual void hold_front_tile() = 0;
     virtual KernelTimer& timer() = 0;
 };
 

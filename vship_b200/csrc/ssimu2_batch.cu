@@ -553,7 +553,8 @@ public:
         while (first < n) {
             LaunchPlan plan = plan_launch(pairs, first, n);
             const int rows = choose_rows(plan, pairs, d_scores, d_features, stream);
-            run(plan, pairs, rows, d_scores, d_features, stream);
+            run(plan, pairs, rows, d_scores, d_features, stream, hold_front_);
+            hold_front_ = false;
             first += plan.count;
         }
     }
@@ -620,6 +621,7 @@ public:
     }
 
     int tile_rows() const override { return last_rows_; }
+    void hold_front_tile() override { hold_front_ = true; }
     KernelTimer& timer() override { return timer_; }
 
 private:
@@ -1023,8 +1025,10 @@ private:
         return graphs_.emplace(key, gr).first->second;
     }
 
+    // hold: launch the front grid without its last tile, so that the map tiles of the last
+    // pair wait for a pyramid that is never finished (the wait-limit test).
     void run(const LaunchPlan& plan, const VshipExt_FramePair* pairs, int rows, double* d_scores, float* d_features,
-             cudaStream_t stream) {
+             cudaStream_t stream, bool hold = false) {
         // The pinned descriptor block is reused: wait until the previous launch has copied it.
         CUDA_CHECK(cudaEventSynchronize(blob_free_));
         int64_t partials = 0;
@@ -1034,7 +1038,7 @@ private:
         Graph& gr = graph_for(rows, path, sizeof(float) * (size_t)plan.stage_floats);
         CUDA_CHECK(cudaGraphExecMemcpyNodeSetParams1D(gr.exec, gr.copy, blob_d_, blob_h_, bytes, cudaMemcpyHostToDevice));
         cudaKernelNodeParams fp = gr.front_params;
-        fp.gridDim = dim3((unsigned)front_total);
+        fp.gridDim = dim3((unsigned)(front_total - (hold ? 1 : 0)));  // front_total >= 2
         CUDA_CHECK(cudaGraphExecKernelNodeSetParams(gr.exec, gr.front, &fp));
         cudaKernelNodeParams tp = gr.tiles_params;
         tp.gridDim = dim3((unsigned)ceil_div(maps_total, 256));
@@ -1089,6 +1093,7 @@ private:
     unsigned* counters_d_ = nullptr;
     int counter_words_ = 0;
     unsigned* err_h_ = nullptr;
+    bool hold_front_ = false;
     float* xyb_ = nullptr;
     int64_t xyb_cap_ = 0;
     double* partials_ = nullptr;
