@@ -80,15 +80,16 @@ __device__ __forceinline__ float load_norm(const uint8_t* plane, int64_t stride,
     return chroma ? (v - 128.f) * (1.0f / 224.f) : (v - 16.f) * (1.0f / 219.f);
 }
 
-// CubicHermitSplineInterpolator (src/gpuColorToLinear/resize.hpp:5-24).
+// CubicHermitSplineInterpolator (src/gpuColorToLinear/resize.hpp:5-24).  Every rounding is
+// spelled out (products by 2 are exact), so the value does not depend on how the compiler
+// fuses multiply-adds in the surrounding code: the per-pixel, quad and staged paths, which
+// share some of these terms, give bit-identical samples.  At t = 0 the result is p0 exactly.
 __device__ __forceinline__ float hermite(float p0, float m0, float p1, float m1, float t) {
-    const float v1 = 2 * p0 + m0 - 2 * p1 + m1;
-    const float v2 = -3 * p0 + 3 * p1 - 2 * m0 - m1;
-    float r = v1;
-    r *= t; r += v2;
-    r *= t; r += m0;
-    r *= t; r += p0;
-    return r;
+    const float v1 = __fadd_rn(__fsub_rn(__fadd_rn(2.f * p0, m0), 2.f * p1), m1);
+    const float v2 = __fsub_rn(__fsub_rn(__fmaf_rn(3.f, p1, __fmul_rn(-3.f, p0)), 2.f * m0), m1);
+    float r = __fmaf_rn(v1, t, v2);
+    r = __fmaf_rn(r, t, m0);
+    return __fmaf_rn(r, t, p0);
 }
 
 // Output sample X of an axis decimated by 2^sub -> interval start i and fraction t.
@@ -197,7 +198,10 @@ __device__ __forceinline__ float ex2_approx(float x) {
 }
 
 __device__ __forceinline__ float fast_pow(float x, float g) { return x > 0.f ? ex2_approx(g * __log2f(x)) : 0.f; }
-__device__ __forceinline__ float signed_powf(float a, float g) { return a < 0 ? -fast_pow(-a, g) : fast_pow(a, g); }
+__device__ __forceinline__ float signed_powf(float a, float g) {
+    const float r = fast_pow(fabsf(a), g);  // one power for either sign
+    return a < 0 ? -r : r;
+}
 
 __device__ __forceinline__ float trc_one(float a, int trc) {
     switch (trc) {
@@ -411,6 +415,20 @@ __device__ __forceinline__ void chroma_stage(const RawImage& im, const ColourPar
         }
     }
     __syncthreads();
+    if constexpr (kFast == kFastYuv420Bt709) {
+        // Co-sited columns (X0 is a multiple of 64): luma columns 2u and 2u + 1 both start at
+        // staged column j = u (hb[2u] = hb[2u + 1] = u) with fractions 0 and 1/2.  At fraction 0
+        // the spline returns its first node exactly (finite samples, never -0), so lane u
+        // writes (S[u + 1], spline at 1/2) as one pair.
+        for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
+            const float* row = st.S + r * kStageMaxSpan + lane;
+            const float em1 = row[0], e0 = row[1], e1 = row[2], e2 = row[3];
+            const float odd = hermite(e0, (e1 - em1) / 2, e1, (e2 - e0) / 2, 0.5f);
+            *reinterpret_cast<float2*>(st.HH + r * kStageTile + 2 * lane) = make_float2(e0, odd);
+        }
+        __syncthreads();
+        return;
+    }
     for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
         const float* row = st.S + r * kStageMaxSpan;
         for (int x = lane; x < kStageTile; x += 32) {
@@ -562,6 +580,63 @@ __device__ __forceinline__ float3 ingest_fast(const RawImage& im, const ColourPa
         v.y = srgb_to_linear(range_luma((float)__ldg(im.p[1] + (int64_t)Y * im.stride[1] + X), cp));
         v.z = srgb_to_linear(range_luma((float)__ldg(im.p[2] + (int64_t)Y * im.stride[2] + X), cp));
         return v;
+    }
+}
+
+// Linear RGB of the 2x2 luma quad at even (X, Y) of a kFastYuv420Bt709 tile with origin
+// (X0, Y0) (also even); `right` / `down` say whether column X + 1 / row Y + 1 exist (the
+// entries of missing pixels hold values read from in-bounds shared memory and must be
+// ignored).  The values equal four ingest_fast calls: with vertically
+// centred 4:2:0 chroma the two luma rows of a quad take chroma rows j .. j + 3 and
+// j + 1 .. j + 4 (fractions 0.75 and 0.25), so each plane reads five shared tap rows, each
+// as one 8-byte load covering both columns.  Luma pairs are read as one 4-byte load when the
+// row is 4-byte aligned.
+__device__ __forceinline__ void ingest_quad_yuv420(const RawImage& im, const ColourParams& cp, const ChromaStage& st,
+                                                   int X, int Y, int X0, int Y0, bool right, bool down, float3 q[4]) {
+    const int x = X - X0, y = Y - Y0;
+    float lum[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        if (r == 1 && !down) break;
+        const unsigned short* row = reinterpret_cast<const unsigned short*>(im.p[0] + (int64_t)(Y + r) * im.stride[0]);
+        unsigned short u0, u1 = 0;
+        if (right && (reinterpret_cast<uintptr_t>(row + X) & 3u) == 0) {
+            const ushort2 u = __ldg(reinterpret_cast<const ushort2*>(row + X));
+            u0 = u.x;
+            u1 = u.y;
+        } else {
+            u0 = __ldg(row + X);
+            if (right) u1 = __ldg(row + X + 1);
+        }
+        lum[2 * r] = range_luma((float)(u0 & cp.mask), cp);
+        lum[2 * r + 1] = range_luma((float)(u1 & cp.mask), cp);
+    }
+    const int nh = st.cy_n * kStageTile;
+    const int j = st.vb[y];
+    const float t0 = st.vt[y], t1 = st.vt[y + 1];
+    float2 c[4];  // pixel (x, y) (x+1, y) (x, y+1) (x+1, y+1) -> (Cb, Cr)
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const float* col = st.HH + p * nh + j * kStageTile + x;
+        float2 h[5];
+#pragma unroll
+        for (int k = 0; k < 4; k++) h[k] = *reinterpret_cast<const float2*>(col + k * kStageTile);
+        h[4] = down ? *reinterpret_cast<const float2*>(col + 4 * kStageTile) : h[3];
+        const float a0 = hermite(h[1].x, (h[2].x - h[0].x) / 2, h[2].x, (h[3].x - h[1].x) / 2, t0);
+        const float a1 = hermite(h[1].y, (h[2].y - h[0].y) / 2, h[2].y, (h[3].y - h[1].y) / 2, t0);
+        const float b0 = hermite(h[2].x, (h[3].x - h[1].x) / 2, h[3].x, (h[4].x - h[2].x) / 2, t1);
+        const float b1 = hermite(h[2].y, (h[3].y - h[1].y) / 2, h[3].y, (h[4].y - h[2].y) / 2, t1);
+        if (p == 0) { c[0].x = a0; c[1].x = a1; c[2].x = b0; c[3].x = b1; }
+        else        { c[0].y = a0; c[1].y = a1; c[2].y = b0; c[3].y = b1; }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float3 v = make_float3(lum[k], c[k].x, c[k].y);
+        v = ncl_to_rgb(v, 0.2126f, 0.0722f);
+        v.x = signed_powf(v.x, 2.4f);
+        v.y = signed_powf(v.y, 2.4f);
+        v.z = signed_powf(v.z, 2.4f);
+        q[k] = v;
     }
 }
 

@@ -52,7 +52,7 @@ struct FrontArgs {
 };
 
 template <bool FromLinear, int kFast>
-__global__ void __launch_bounds__(256) ssimu2_front_kernel(const __grid_constant__ FrontArgs a) {
+__global__ void __launch_bounds__(256, 4) ssimu2_front_kernel(const __grid_constant__ FrontArgs a) {
     __shared__ FrontSmem fs;
     extern __shared__ float stage_mem[];
     const int img = blockIdx.z;

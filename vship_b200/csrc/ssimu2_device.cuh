@@ -162,10 +162,20 @@ __device__ __forceinline__ void front_tile(FrontSmem& fs, float* stage_mem, cons
         if (gx >= W1 || gy >= H1) continue;
         const int X0 = 2 * gx, Y0 = 2 * gy;
         const int X1 = min(X0 + 1, W0 - 1), Y1 = min(Y0 + 1, H0 - 1);
-        const float3 p00 = pixel(X0, Y0);
-        const float3 p01 = (X1 != X0) ? pixel(X1, Y0) : p00;
-        const float3 p10 = (Y1 != Y0) ? pixel(X0, Y1) : p00;
-        const float3 p11 = (Y1 != Y0) ? ((X1 != X0) ? pixel(X1, Y1) : p10) : p01;
+        float3 p00, p01, p10, p11;
+        if constexpr (!FromLinear && kFast == kFastYuv420Bt709) {
+            float3 q4[4];
+            ingest_quad_yuv420(im, cp, st, X0, Y0, X0t, Y0t, X1 != X0, Y1 != Y0, q4);
+            p00 = q4[0];
+            p01 = (X1 != X0) ? q4[1] : p00;
+            p10 = (Y1 != Y0) ? q4[2] : p00;
+            p11 = (Y1 != Y0) ? ((X1 != X0) ? q4[3] : p10) : p01;
+        } else {
+            p00 = pixel(X0, Y0);
+            p01 = (X1 != X0) ? pixel(X1, Y0) : p00;
+            p10 = (Y1 != Y0) ? pixel(X0, Y1) : p00;
+            p11 = (Y1 != Y0) ? ((X1 != X0) ? pixel(X1, Y1) : p10) : p01;
+        }
         // Level-0 XYB: only the Y plane has unpruned maps at full resolution.
         if (!kCoarse) {
         const float y00 = positive_xyb(p00).y;
