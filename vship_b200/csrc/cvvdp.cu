@@ -123,6 +123,27 @@ __global__ void __launch_bounds__(256, 3) cv_ingest_kernel(const __grid_constant
     ChromaStage st{};
     if (cp.subw || cp.subh) chroma_stage<kFast>(p.im[k], cp, X0, Y0, stage_mem, st);
     float* out = p.slot[k];
+    if constexpr (kFast == kFastYuv420Bt709) {
+        // One 2x2 quad per work item: the quad's chroma rows and luma pairs are read together
+        // (ingest_quad_yuv420), the same values as four single-pixel reads.
+        for (int q = threadIdx.x; q < kStageTile * kStageTile / 4; q += blockDim.x) {
+            const int X = X0 + 2 * (q & (kStageTile / 2 - 1)), Y = Y0 + 2 * (q / (kStageTile / 2));
+            if (X >= cp.W || Y >= cp.H) continue;
+            const bool right = X + 1 < cp.W, down = Y + 1 < cp.H;
+            float3 lin[4];
+            ingest_quad_yuv420(p.im[k], cp, st, X, Y, X0, Y0, right, down, lin);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                if (((e & 1) && !right) || ((e & 2) && !down)) continue;
+                const float3 v = encode_pixel(lin[e], p.disp, p.trc[k], p.prim[k]);
+                const int64_t o = (int64_t)(Y + (e >> 1)) * cp.W + X + (e & 1);
+                out[o] = v.x;
+                out[p.n + o] = v.y;
+                out[2 * p.n + o] = v.z;
+            }
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < kStageTile * kStageTile; i += blockDim.x) {
         const int X = X0 + (i & (kStageTile - 1)), Y = Y0 + i / kStageTile;
         if (X >= cp.W || Y >= cp.H) continue;
