@@ -197,7 +197,21 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
-__device__ __forceinline__ float fast_pow(float x, float g) { return x > 0.f ? ex2_approx(g * __log2f(x)) : 0.f; }
+// log2 on the special-function unit without the subnormal-input fix-up (PTX
+// lg2.approx.ftz: a subnormal input reads as 0 and gives -inf; normal inputs give the same
+// value as lg2.approx).
+__device__ __forceinline__ float lg2_ftz(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// x^g for x > 0 (0 otherwise) as exp2(g log2 x).  Every caller passes g >= 1, where a
+// subnormal x gives 0 through the flushed log2 (-inf) just as through the exact one (the
+// power underflows and exp2 flushes it), or an x that is never subnormal (sRGB above its
+// knee, ST 240 above 0.0228); so the flushed log2 gives the same values with fewer
+// instructions.
+__device__ __forceinline__ float fast_pow(float x, float g) { return x > 0.f ? ex2_approx(g * lg2_ftz(x)) : 0.f; }
 __device__ __forceinline__ float signed_powf(float a, float g) {
     const float r = fast_pow(fabsf(a), g);  // one power for either sign
     return a < 0 ? -r : r;
