@@ -354,14 +354,14 @@ __global__ void __launch_bounds__(kMapThreads, TH == 64 ? 3 : 4) ssimu2_batch_ma
     unsigned partial = e0.z;
     gate.wait(v, pair);
     typename MT::Regs regs;
-    load_halo<TH, true>(cur, regs);
+    load_halo<TH, true, false>(cur, regs);
     bool have = true;
     for (;;) {
         if (!have) {
             gate.wait(v, pair);
-            load_halo<TH, true>(cur, regs);
+            load_halo<TH, true, false>(cur, regs);
         }
-        stage_halo<TH>(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
+        stage_halo<TH, false>(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
         const TileRef t = cur;
         const unsigned tpartial = partial;
         const int next = m + stride;
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kMapThreads, TH == 64 ? 3 : 4) ssimu2_batch_ma
             // Prefetch only when the next pair's pyramids are complete; otherwise wait after
             // this tile (never while holding it).
             if (gate.ready(v, pair)) {
-                load_halo<TH, true>(cur, regs);
+                load_halo<TH, true, false>(cur, regs);
                 have = true;
             }
         }
