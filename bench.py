@@ -38,7 +38,7 @@ WORKLOAD = "ssimu2_1080p_yuv420p10_bt709_batch64"
 METRIC = "1080p SSIMU2 frame-pairs/s"
 UNIT = "frame-pairs/s"
 
-# Algorithmic bytes per 1080p pair (see DESIGN.md "Roofline"): the front kernel reads the
+# Algorithmic bytes per 1080p pair: the front kernel reads the
 # raw 10-bit 4:2:0 planes of both frames and writes the XYB planes the maps read; the maps
 # kernel reads those planes once.
 RAW_BYTES_PER_IMAGE = 1920 * 1080 * 2 + 2 * 960 * 540 * 2
@@ -48,6 +48,21 @@ ALGO_BYTES = {
     "ssimu2_maps": 2 * 4 * XYB_FLOATS_PER_IMAGE,
     "ssimu2_final": 0,
 }
+
+
+def maps_flop_per_pair(w, h):
+    """FP32 arithmetic of the maps kernel for one pair: every unpruned (plane, level) is cut into
+    32 x 32 output tiles, and each output position costs ~370 FLOP (the horizontal 17-tap pass
+    over 1.5x the rows for four moment inputs, 204; the vertical pass, 136; the maps, ~30)."""
+    planes = [1, 2, 2, 3, 3]  # Y at level 0; X, Y at 1-2; X, Y, B at 3-4; level 5 pruned
+    tiles = 0
+    for n in planes:
+        tiles += n * (-(-w // 32)) * (-(-h // 32))
+        w, h = (w - 1) // 2 + 1, (h - 1) // 2 + 1
+    return tiles * 1024 * 370
+
+
+FP32_NOMINAL_TFLOPS = 80.0  # B200 FP32 SIMT, nominal
 
 
 def log(*a):
@@ -213,6 +228,14 @@ def run_ours(args, world, rank, local):
                 "traffic": None, "algorithmic_bytes_per_launch": ALGO_BYTES[top_name] * BATCH,
                 "avg_launch_ms": round(avg_ms, 4),
                 "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in ktimes.items()}}
+    if top_name == "ssimu2_maps":
+        # The maps kernel is arithmetic-bound (47 FLOP per algorithmic byte, far right of the
+        # FP32 ridge): its compute fraction is the descriptive figure.
+        flop = maps_flop_per_pair(W, H) * BATCH
+        tf = flop / (avg_ms / 1e3) / 1e12
+        roofline["compute"] = {"flop_per_launch": flop, "achieved_tflops": round(tf, 2),
+                               "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_source": "nominal FP32 SIMT",
+                               "frac": round(tf / FP32_NOMINAL_TFLOPS, 4)}
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
@@ -381,7 +404,9 @@ def run_reference(args, world, rank, local):
 BW, BH, BBATCH = 3840, 2160, 32
 BWORKLOAD = "butteraugli_4k_srgb8_batch32_q5_i203_distmap"
 BMETRIC = "4K Butteraugli frame-pairs/s"
-# Algorithmic bytes per 4K Butteraugli pair (FP32 staged model, see DESIGN.md "Roofline").
+# Algorithmic bytes per 4K Butteraugli pair (FP32 staged model: inputs, then per scale every
+# opsin and band plane of both images written and read once, the accumulator and mask planes
+# written and read, the per-scale diff map, and the final distortion map written).
 B_ALGO_BYTES = 2_903_040_000
 
 

@@ -5,8 +5,9 @@
  * Each declaration below replaces the reference declaration cited beside it
  * (Line-fr/Vship 4.1.0, src/VshipAPI.h).  Names, argument order, types and enum values are
  * ABI-identical so that FFVship, VapourSynth scripts and other callers of the reference
- * library link against this one unchanged.  Behaviour differences, if any, are listed in
- * DESIGN.md of this repository.
+ * library link against this one unchanged.  Behaviour differences: a freed or never-
+ * initialised handler id returns Vship_BadHandler (undefined behaviour in the reference), and
+ * device memory is taken at Init rather than per frame.
  *
  * Threading contract (same as the reference): any number of handlers may be used from
  * different threads at the same time; one handler must not be used by two threads at once

@@ -2,7 +2,7 @@
 //
 // Mirrors src/VshipLib.cpp:70-562 of the reference: handler tables with reusable ids, a
 // global and a per-handler last error, the same error codes and message layout.  The
-// differences are deliberate and listed in DESIGN.md: a freed or never-initialised id gives
+// differences are deliberate: a freed or never-initialised id gives
 // Vship_BadHandler instead of undefined behaviour, a handler used by two threads at once
 // gives Vship_BadHandler instead of a data race, and the global last error is guarded by a
 // mutex.
