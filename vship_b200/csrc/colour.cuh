@@ -81,15 +81,36 @@ __device__ __forceinline__ float load_norm(const uint8_t* plane, int64_t stride,
 }
 
 // CubicHermitSplineInterpolator (src/gpuColorToLinear/resize.hpp:5-24).  Every rounding is
-// spelled out (products by 2 are exact), so the value does not depend on how the compiler
-// fuses multiply-adds in the surrounding code: the per-pixel, quad and staged paths, which
-// share some of these terms, give bit-identical samples.  At t = 0 the result is p0 exactly.
+// spelled out, so the value does not depend on how the compiler fuses multiply-adds in the
+// surrounding code: the per-pixel, quad and staged paths, which share some of these terms,
+// give bit-identical samples.  Products by +-2 are exact, so fma(+-2, x, y) rounds exactly as
+// y +- 2x does, in one instruction.  At t = 0 the result is p0 exactly.
 __device__ __forceinline__ float hermite(float p0, float m0, float p1, float m1, float t) {
-    const float v1 = __fadd_rn(__fsub_rn(__fadd_rn(2.f * p0, m0), 2.f * p1), m1);
-    const float v2 = __fsub_rn(__fsub_rn(__fmaf_rn(3.f, p1, __fmul_rn(-3.f, p0)), 2.f * m0), m1);
+    const float v1 = __fadd_rn(__fmaf_rn(-2.f, p1, __fmaf_rn(2.f, p0, m0)), m1);
+    const float v2 = __fsub_rn(__fmaf_rn(-2.f, m0, __fmaf_rn(3.f, p1, __fmul_rn(-3.f, p0))), m1);
     float r = __fmaf_rn(v1, t, v2);
     r = __fmaf_rn(r, t, m0);
     return __fmaf_rn(r, t, p0);
+}
+
+// hermite() on two independent lanes with packed FP32x2 arithmetic of sm_100: every lane
+// takes hermite()'s operations in hermite()'s order (x - y as x + (-y), which rounds the
+// same), so each lane equals the scalar call bit for bit.
+__device__ __forceinline__ float2 hermite2(float2 p0, float2 m0, float2 p1, float2 m1, float t) {
+    const float2 two = make_float2(2.f, 2.f), mtwo = make_float2(-2.f, -2.f);
+    const float2 v1 = __fadd2_rn(__ffma2_rn(mtwo, p1, __ffma2_rn(two, p0, m0)), m1);
+    const float2 v2 = __fadd2_rn(
+        __ffma2_rn(mtwo, m0, __ffma2_rn(make_float2(3.f, 3.f), p1, __fmul2_rn(make_float2(-3.f, -3.f), p0))),
+        make_float2(-m1.x, -m1.y));
+    const float2 tt = make_float2(t, t);
+    float2 r = __ffma2_rn(v1, tt, v2);
+    r = __ffma2_rn(r, tt, m0);
+    return __ffma2_rn(r, tt, p0);
+}
+
+// Central-difference tangent (b - a) / 2 of two lanes, rounded as the scalar expression.
+__device__ __forceinline__ float2 tangent2(float2 a, float2 b) {
+    return __fmul2_rn(__fadd2_rn(b, make_float2(-a.x, -a.y)), make_float2(0.5f, 0.5f));
 }
 
 // Output sample X of an axis decimated by 2^sub -> interval start i and fraction t.
@@ -636,10 +657,11 @@ __device__ __forceinline__ void ingest_quad_yuv420(const RawImage& im, const Col
 #pragma unroll
         for (int k = 0; k < 4; k++) h[k] = *reinterpret_cast<const float2*>(col + k * kStageTile);
         h[4] = down ? *reinterpret_cast<const float2*>(col + 4 * kStageTile) : h[3];
-        const float a0 = hermite(h[1].x, (h[2].x - h[0].x) / 2, h[2].x, (h[3].x - h[1].x) / 2, t0);
-        const float a1 = hermite(h[1].y, (h[2].y - h[0].y) / 2, h[2].y, (h[3].y - h[1].y) / 2, t0);
-        const float b0 = hermite(h[2].x, (h[3].x - h[1].x) / 2, h[3].x, (h[4].x - h[2].x) / 2, t1);
-        const float b1 = hermite(h[2].y, (h[3].y - h[1].y) / 2, h[3].y, (h[4].y - h[2].y) / 2, t1);
+        // Both columns at once: lane .x is column x, lane .y column x + 1.
+        const float2 g1 = tangent2(h[0], h[2]), g2 = tangent2(h[1], h[3]), g3 = tangent2(h[2], h[4]);
+        const float2 av = hermite2(h[1], g1, h[2], g2, t0);
+        const float2 bv = hermite2(h[2], g2, h[3], g3, t1);
+        const float a0 = av.x, a1 = av.y, b0 = bv.x, b1 = bv.y;
         if (p == 0) { c[0].x = a0; c[1].x = a1; c[2].x = b0; c[3].x = b1; }
         else        { c[0].y = a0; c[1].y = a1; c[2].y = b0; c[3].y = b1; }
     }
