@@ -624,8 +624,9 @@ __device__ __forceinline__ float3 ingest_fast(const RawImage& im, const ColourPa
 // ignored).  The values equal four ingest_fast calls: with vertically
 // centred 4:2:0 chroma the two luma rows of a quad take chroma rows j .. j + 3 and
 // j + 1 .. j + 4 (fractions 0.75 and 0.25), so each plane reads five shared tap rows, each
-// as one 8-byte load covering both columns.  Luma pairs are read as one 4-byte load when the
-// row is 4-byte aligned.
+// as one 8-byte load covering both columns, and interpolates both columns of a luma row with
+// one packed spline (hermite2).  Luma pairs are read as one 4-byte load when the row is
+// 4-byte aligned.
 __device__ __forceinline__ void ingest_quad_yuv420(const RawImage& im, const ColourParams& cp, const ChromaStage& st,
                                                    int X, int Y, int X0, int Y0, bool right, bool down, float3 q[4]) {
     const int x = X - X0, y = Y - Y0;
