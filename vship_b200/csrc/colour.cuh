@@ -409,36 +409,61 @@ __device__ __forceinline__ void chroma_stage(const RawImage& im, const ColourPar
         st.vt[tid - kStageTile] = f;
     }
     const bool chroma = cp.yuv_chroma != 0;
-    if constexpr (kFast == kFastYuv420Bt709) {  // aligned 16-bit samples, cx_n <= 36 columns
-        constexpr int kBatch = 19;
-        const int c = tid & 63, ng = blockDim.x >> 6, rows = 2 * st.cy_n;
-        if (c < st.cx_n) {
-            const int gx = min(max(st.cx_lo + c, 0), cw - 1);
-            for (int r0 = tid >> 6; r0 < rows; r0 += ng * kBatch) {
-                unsigned short u[kBatch];
+    if constexpr (kFast == kFastYuv420Bt709) {
+        // Aligned 16-bit samples, co-sited columns (X0 is a multiple of 64): luma columns 2u and
+        // 2u + 1 both start at staged column u with fractions 0 and 1/2, and at fraction 0 the
+        // spline returns its first node exactly (finite samples, never -0).  Lane u of a warp
+        // holds staged samples u and, for u < 3, 32 + u of each of its rows; it reads samples
+        // u + 1 .. u + 3 from its neighbours by shuffles and writes HH columns (2u, 2u + 1) as
+        // one pair.  Raw samples never pass through shared memory, and all of a warp's row
+        // loads are issued before any is used.
+        constexpr int kRowsPerWarp = 10;  // 2 x 37 staged rows over 8 warps
+        const int rows = 2 * st.cy_n;
+        const int gx_lo = min(max(st.cx_lo + lane, 0), cw - 1);
+        const int gx_hi = min(max(st.cx_lo + 32 + min(lane, 2), 0), cw - 1);
+        for (int base = warp; base < rows; base += nwarps * kRowsPerWarp) {
+            unsigned lo[kRowsPerWarp], hi[kRowsPerWarp];
 #pragma unroll
-                for (int k = 0; k < kBatch; k++) {
-                    const int r = r0 + k * ng;
-                    u[k] = 0;
-                    if (r < rows) {
-                        const int p = r >= st.cy_n, rr = r - p * st.cy_n;
-                        const int gy = min(max(st.cy_lo + rr, 0), ch - 1);
-                        u[k] = __ldg(reinterpret_cast<const unsigned short*>(im.p[1 + p] + (int64_t)gy * im.stride[1 + p]) + gx);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < kBatch; k++) {
-                    const int r = r0 + k * ng;
-                    if (r < rows) {
-                        float v = (float)(u[k] & cp.mask);
-                        // FullRange of a chroma sample, as load_norm computes it.
-                        if (cp.full_range) v = v * cp.full_scale - 0.5f;
-                        else v = (v * cp.lim_scale - 128.f) * (1.0f / 224.f);
-                        st.S[r * kStageMaxSpan + c] = v;
-                    }
+            for (int k = 0; k < kRowsPerWarp; k++) {
+                const int r = base + k * nwarps;
+                lo[k] = hi[k] = 0u;
+                if (r < rows) {
+                    const int p = r >= st.cy_n, rr = r - p * st.cy_n;
+                    const int gy = min(max(st.cy_lo + rr, 0), ch - 1);
+                    const unsigned short* src =
+                        reinterpret_cast<const unsigned short*>(im.p[1 + p] + (int64_t)gy * im.stride[1 + p]);
+                    lo[k] = __ldg(src + gx_lo);
+                    hi[k] = __ldg(src + gx_hi);
                 }
             }
+#pragma unroll
+            for (int k = 0; k < kRowsPerWarp; k++) {
+                const int r = base + k * nwarps;
+                if (r >= rows) break;  // the same for every lane of the warp
+                float a = (float)(lo[k] & cp.mask), b = (float)(hi[k] & cp.mask);
+                // FullRange of a chroma sample, as load_norm computes it.
+                if (cp.full_range) {
+                    a = a * cp.full_scale - 0.5f;
+                    b = b * cp.full_scale - 0.5f;
+                } else {
+                    a = (a * cp.lim_scale - 128.f) * (1.0f / 224.f);
+                    b = (b * cp.lim_scale - 128.f) * (1.0f / 224.f);
+                }
+                float e[4];
+                e[0] = a;
+#pragma unroll
+                for (int d = 1; d < 4; d++) {
+                    const int src_lane = (lane + d) & 31;
+                    const float va = __shfl_sync(0xffffffffu, a, src_lane);
+                    const float vb = __shfl_sync(0xffffffffu, b, src_lane);
+                    e[d] = lane + d < 32 ? va : vb;
+                }
+                const float odd = hermite(e[1], (e[2] - e[0]) / 2, e[2], (e[3] - e[1]) / 2, 0.5f);
+                *reinterpret_cast<float2*>(st.HH + r * kStageTile + 2 * lane) = make_float2(e[1], odd);
+            }
         }
+        __syncthreads();
+        return;
     } else {
         for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
             const int p = r >= st.cy_n, rr = r - p * st.cy_n;
@@ -450,20 +475,6 @@ __device__ __forceinline__ void chroma_stage(const RawImage& im, const ColourPar
         }
     }
     __syncthreads();
-    if constexpr (kFast == kFastYuv420Bt709) {
-        // Co-sited columns (X0 is a multiple of 64): luma columns 2u and 2u + 1 both start at
-        // staged column j = u (hb[2u] = hb[2u + 1] = u) with fractions 0 and 1/2.  At fraction 0
-        // the spline returns its first node exactly (finite samples, never -0), so lane u
-        // writes (S[u + 1], spline at 1/2) as one pair.
-        for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
-            const float* row = st.S + r * kStageMaxSpan + lane;
-            const float em1 = row[0], e0 = row[1], e1 = row[2], e2 = row[3];
-            const float odd = hermite(e0, (e1 - em1) / 2, e1, (e2 - e0) / 2, 0.5f);
-            *reinterpret_cast<float2*>(st.HH + r * kStageTile + 2 * lane) = make_float2(e0, odd);
-        }
-        __syncthreads();
-        return;
-    }
     for (int r = warp; r < 2 * st.cy_n; r += nwarps) {
         const float* row = st.S + r * kStageMaxSpan;
         for (int x = lane; x < kStageTile; x += 32) {
