@@ -318,10 +318,11 @@ __device__ __forceinline__ float3 primaries_to_709(float3 v, int prim) {
 
 // ---------------------------------------------------------------------------------------
 // Tile-staged chroma: a CTA working on luma tile [X0, X0+64) x [Y0, Y0+64) decodes each
-// chroma sample it needs once into shared memory (S, with the edge replication of the
-// reference's clamped interpolators baked in), interpolates horizontally once per (chroma
-// row, luma column) into HH, and every pixel then does only the vertical step.  Interval
-// starts and fractions of the tile's 64 columns and rows come from small phase tables.
+// chroma sample it needs once, with the edge replication of the reference's clamped
+// interpolators baked in (into shared memory S, or, on the 10-bit 4:2:0 path, into registers
+// shared within a warp by shuffles), interpolates horizontally once per (chroma row, luma
+// column) into HH, and every pixel then does only the vertical step.  Interval starts and
+// fractions of the tile's 64 columns and rows come from small phase tables.
 // ---------------------------------------------------------------------------------------
 constexpr int kStageTile = 64;
 // Front paths (see fast_path_of): the generic runtime-dispatched one and two compile-time ones.
@@ -331,7 +332,8 @@ constexpr int kStageMaxSpan = kStageTile + 4;  // staged rows/columns: interval 
 struct ChromaStage {
     int cx_lo, cx_n;     // staged chroma columns [cx_lo, cx_lo + cx_n) (may start below 0)
     int cy_lo, cy_n;     // staged chroma rows
-    float* S;            // [2][cy_n][kStageMaxSpan] decoded, range-normalised samples
+    float* S;            // [2][cy_n][kStageMaxSpan] decoded, range-normalised samples (not
+                         // used by the 10-bit 4:2:0 path)
     float* HH;           // [2][cy_n][64] horizontally interpolated at each luma column
     short* hb;           // [64] S column of the first tap of luma column x
     float* ht;           // [64] horizontal fraction of luma column x
