@@ -21,17 +21,61 @@ _lib = None
 
 def build(force=False):
     """Compile oracle.c (gcc, OpenMP).  Needs only gcc; runs here and on the GPU box."""
-    srcs = [os.path.join(HERE, "oracle.c"), os.path.join(HERE, "cvvdp.c")]
+    srcs = [os.path.join(HERE, "oracle.c"), os.path.join(HERE, "cvvdp.c"), os.path.join(HERE, "ssimu2_f32.c")]
     csrc = os.path.join(os.path.dirname(HERE), "vship_b200", "csrc")
     deps = srcs + [os.path.join(csrc, "metric_tables.h"), os.path.join(csrc, "cvvdp_csf_table.h")]
     if (not force and os.path.exists(LIB_PATH)
             and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(d) for d in deps)):
         return LIB_PATH
     tmp = LIB_PATH + ".tmp"
-    subprocess.check_call(["gcc", "-O2", "-fopenmp", "-shared", "-fPIC", "-std=c11",
+    subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-shared", "-fPIC", "-std=c11",
                            "-fvisibility=hidden", "-o", tmp] + srcs + ["-lm"])
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
+
+
+CUDA_MATH_PATH = os.path.join(HERE, "libcudamath.so")
+_cuda_math = None
+
+
+def build_cuda_math(force=False):
+    """Compile cuda_math.cu (CUDA's own powf/cbrtf/expf over arrays) with nvcc's default math
+    flags, as the reference library is built.  Test infrastructure only."""
+    src = os.path.join(HERE, "cuda_math.cu")
+    if not force and os.path.exists(CUDA_MATH_PATH) and os.path.getmtime(CUDA_MATH_PATH) >= os.path.getmtime(src):
+        return CUDA_MATH_PATH
+    tmp = CUDA_MATH_PATH + ".tmp"
+    subprocess.check_call(["nvcc", "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+                           "-Xcompiler", "-fPIC", "-o", tmp, src])
+    os.replace(tmp, CUDA_MATH_PATH)
+    return CUDA_MATH_PATH
+
+
+_MATH_FN = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_float,
+                            ctypes.POINTER(ctypes.c_float), ctypes.c_int64)
+
+
+def use_cuda_math(enable=True):
+    """Make the FP32 restatement take powf/cbrtf/expf from CUDA on the current GPU (True) or
+    from the correctly rounded CPU evaluation (False)."""
+    global _cuda_math
+    L = lib()
+    if not enable:
+        L.oracle_f32_set_math(ctypes.cast(None, _MATH_FN))
+        _cuda_math = None
+        return
+    cm = ctypes.CDLL(build_cuda_math())
+    cm.cm_eval.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.c_float,
+                           ctypes.POINTER(ctypes.c_float), ctypes.c_int64]
+    cm.cm_eval.restype = ctypes.c_int
+
+    def _eval(op, x, y, out, n):
+        rc = cm.cm_eval(op, x, y, out, n)
+        if rc != 0:
+            raise RuntimeError("cm_eval failed with CUDA error %d" % rc)
+
+    _cuda_math = (cm, _MATH_FN(_eval))   # keep the callback alive
+    L.oracle_f32_set_math(_cuda_math[1])
 
 
 def build_reference():
@@ -60,6 +104,15 @@ def lib():
         L.oracle_downsample.argtypes = [dp, ctypes.c_int64, ctypes.c_int64, dp]
         L.oracle_positive_xyb.argtypes = [dp, ctypes.c_int64]
         L.oracle_num_threads.restype = ctypes.c_int
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.oracle_f32_convert.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int64),
+                                         ctypes.POINTER(abi.Colorspace), fp]
+        L.oracle_f32_convert.restype = ctypes.c_int
+        L.oracle_f32_ssimu2.argtypes = [fp, fp, ctypes.c_int64, ctypes.c_int64, fp]
+        L.oracle_f32_ssimu2.restype = ctypes.c_double
+        L.oracle_f32_set_variant.argtypes = [ctypes.c_int]
+        L.oracle_f32_set_math.argtypes = [_MATH_FN]
+        L.oracle_f32_get_variant.restype = ctypes.c_int
         L.oracle_convert_native.argtypes = L.oracle_convert.argtypes
         L.oracle_convert_native.restype = ctypes.c_int
         vp, i64 = ctypes.c_void_p, ctypes.c_int64
@@ -185,6 +238,39 @@ def ssimu2(rgb1, rgb2):
     d = ctypes.c_double()
     lib().oracle_ssimu2(_dp(rgb1), _dp(rgb2), w, h, _dp(feats), ctypes.byref(q), ctypes.byref(d))
     return q.value, d.value, feats
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def convert_f32(planes, line_sizes, cs):
+    """Raw planes -> planar linear BT.709 RGB in the reference's own float arithmetic
+    (ssimu2_f32.c), float32 (3, H, W)."""
+    ow, oh = cs.out_dims()
+    out = np.empty((3, oh, ow), dtype=np.float32)
+    bufs = [np.ascontiguousarray(np.frombuffer(memoryview(p), dtype=np.uint8)) for p in planes]
+    ptrs = (ctypes.c_void_p * 3)(*[b.ctypes.data for b in bufs])
+    ls = (ctypes.c_int64 * 3)(*line_sizes)
+    if lib().oracle_f32_convert(ptrs, ls, ctypes.byref(cs), _fp(out)) != 0:
+        raise ValueError("unsupported chroma subsampling")
+    return out
+
+
+def ssimu2_f32(rgb1, rgb2):
+    """SSIMULACRA2 of two float32 (3, H, W) linear RGB images with the reference's float
+    arithmetic (ssimu2_f32.c).  Returns (score, 108 float features)."""
+    rgb1 = np.ascontiguousarray(rgb1, dtype=np.float32)
+    rgb2 = np.ascontiguousarray(rgb2, dtype=np.float32)
+    _, h, w = rgb1.shape
+    feats = np.zeros(108, dtype=np.float32)
+    score = lib().oracle_f32_ssimu2(_fp(rgb1), _fp(rgb2), w, h, _fp(feats))
+    return score, feats
+
+
+def ssimu2_reference_arith(p1, ls1, cs1, p2, ls2, cs2):
+    """Score of a raw frame pair as the reference library's float pipeline forms it."""
+    return ssimu2_f32(convert_f32(p1, ls1, cs1), convert_f32(p2, ls2, cs2))[0]
 
 
 def ssimu2_final(features, quirk=True):

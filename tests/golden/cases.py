@@ -133,3 +133,29 @@ CASES = [
          crop=[2, 2, 4, 4]),
     dict(name="b_identity_pad", metric=B, w=160, h=96, seed=38, identical=True, qnorm=5, intensity=165.0, pad=[7, 7, 7]),
 ]
+
+
+def _variant(base, **over):
+    c = dict(next(c for c in CASES if c["name"] == base))
+    c.update(over)
+    return c
+
+
+# Every SSIMULACRA2-only colour path again at >= 60k pixels (where the reference's float
+# drift is small) and as Butteraugli cases (no cancellation: the colour path is pinned to
+# the reference's own outputs at 1e-5).
+_COLOUR_PATHS = ["s_yuv422p8_center_170m", "s_yuv410_topleft_12bit", "s_yuv411_center_9bit",
+                 "s_yuv420_top_14bit_2020cl", "s_yuv444p16_2020ncl_pq", "s_ictcp_pq_half", "s_yuv_hlg_float",
+                 "s_rgb_float_linear_xyz", "s_rgb16_st428", "s_rgb8_limited_srgb"]
+_SIZES = {"s_yuv411_center_9bit": (301, 221), "s_yuv410_topleft_12bit": (340, 200), "s_yuv422p8_center_170m": (352, 240)}
+CASES += [_variant(n, name=n + "_big", seed=100 + k, w=_SIZES.get(n, (320, 240))[0], h=_SIZES.get(n, (320, 240))[1])
+          for k, n in enumerate(_COLOUR_PATHS)]
+CASES += [
+    dict(name="s_resize_crop_big", metric=S, w=400, h=260, seed=120, step=16.0, tw=360, th=220, crop=[2, 4, 6, 8]),
+    dict(name="s_crop_only_big", metric=S, w=340, h=240, seed=121, step=16.0, crop=[10, 10, 10, 10]),
+    dict(name="s_upscale_big", metric=S, w=256, h=192, seed=122, step=16.0, tw=384, th=256),
+]
+CASES += [_variant(n, name="b" + n[1:], metric=B, seed=140 + k, w=128, h=96, qnorm=5 if k % 2 else 3,
+                   intensity=203.0 if k % 3 else 80.0)
+          for k, n in enumerate(_COLOUR_PATHS + ["s_crop_only"])]
+CASES += [_variant("s_upscale", name="b_upscale", metric=B, seed=152, w=90, h=64, tw=128, th=96, qnorm=5, intensity=203.0)]

@@ -166,31 +166,32 @@ def _golden():
 
 
 def test_oracle_matches_reference_golden_ssimu2(oracle_lib):
-    """Pin of the SSIMULACRA2 restatement against the reference's own outputs.
+    """FP64 restatement against the reference's own scores on full-HD frames.
 
     The reference evaluates the SSIM map in FP32 as 1 - num/den with variances formed as
     blur((a+b)^2) - 2 blur(ab) - mu^2 (src/ssimu2/score.hpp:232-274); in smooth regions that
-    cancels ~1e-4 of rounding noise into a map whose values are ~1e-4, and max(., 0) turns the
-    noise into a bias.  Its scores therefore drift from the exact metric by ~1e-3 on frames of
-    60k+ pixels (2e-3 at 1080p) and by up to ~1 on frames of a few pixels (on identical
-    720x480 content it returns 99.89, not 100).  The pin is taken where that drift is below
-    the metric's resolution; the pixel counts and tolerance are stated here."""
+    cancels rounding noise into a map whose values are ~1e-4, and max(., 0) turns the noise
+    into a bias.  ssimu2_f32.c reproduces the reference's scores bit for bit from the
+    reference's own float arithmetic (tests/test_reference_arith_gpu.py), so the difference
+    between the exact metric and the reference is that float arithmetic; it is ~1e-3 on
+    full-HD frames and grows as frames shrink (up to ~1 on a few pixels).  This test bounds it
+    where it is smallest: frames of 2 Mpixels, within 2e-3."""
     from tests.golden.cases import build_case
     data = _golden()
     checked = 0
     for case in data["cases"]:
-        if case["metric"] != "ssimu2" or case.get("identical") or not (60_000 <= case["w"] * case["h"] <= 2_100_000):
+        if case["metric"] != "ssimu2" or case.get("identical") or not (1_000_000 <= case["w"] * case["h"] <= 2_100_000):
             continue
         (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
         q, d, _ = oracle_lib.ssimu2(oracle_lib.convert(p1, ls1, cs1), oracle_lib.convert(p2, ls2, cs2))
         assert abs(d - case["score"]) <= 2e-3, (case["name"], d, case["score"])
         checked += 1
-    assert checked >= 4
+    assert checked >= 3
 
 
 def test_reference_fp32_drift_shrinks_with_size(oracle_lib):
     """The reference/FP64 gap is rounding noise, not an algorithm difference: it is largest
-    on a few pixels and small at full HD for every colourspace of the golden set."""
+    on a few pixels and small at full HD."""
     from tests.golden.cases import build_case
     data = _golden()
     gaps = {}
@@ -205,23 +206,69 @@ def test_reference_fp32_drift_shrinks_with_size(oracle_lib):
     assert max(gaps.values()) < 1.0
 
 
-def test_oracle_matches_reference_golden_butteraugli(oracle_lib):
-    """Butteraugli has no such cancellation: the restatement matches the reference's norms
-    to 1e-5 relative and its distortion map samples to 1e-4."""
+def test_fp32_restatement_tracks_reference_where_fp64_cannot(oracle_lib):
+    """ssimu2_f32.c repeats the reference's float arithmetic; on the CPU its powf / cbrtf /
+    expf values are the correctly rounded ones, which CUDA's own functions match for most but
+    not all arguments, and one differing bit moves the score of a tiny frame by up to ~0.1.
+    Even so it lands within 5e-3 of the reference's 94.436943 on the 2x3 sRGB frame, which
+    the exact metric misses by 0.96, and within 1e-4 of the reference's 99.887573 on the
+    identity case, which the exact metric scores 100.  With CUDA's own functions it matches
+    every case exactly (tests/test_reference_arith_gpu.py)."""
     from tests.golden.cases import build_case
+    data = {c["name"]: c for c in _golden()["cases"]}
+    for name, tol in (("s_rgb8_2x3", 5e-3), ("s_identity_yuv420p10_pad", 1e-4)):
+        case = data[name]
+        (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
+        got = oracle_lib.ssimu2_reference_arith(p1, ls1, cs1, p2, ls2, cs2)
+        _, exact, _ = oracle_lib.ssimu2(oracle_lib.convert(p1, ls1, cs1), oracle_lib.convert(p2, ls2, cs2))
+        assert abs(got - case["score"]) <= tol, (name, got, case["score"])
+        assert abs(exact - case["score"]) > 10 * tol, (name, exact, case["score"])
+
+
+def _butteraugli_cases():
     data = _golden()
+    return [c for c in data["cases"] if c["metric"] == "butteraugli" and c["w"] * c["h"] <= 600_000]
+
+
+# The two PQ colour paths, where the reference's FP32 transfer and ICtCp matrices move the
+# linear values of dark pixels by ~1e-4 (the PQ EOTF raises V^(1/m) - c1 to 1/n ~ 6.3).
+_FP32_COLOUR_SENSITIVE = {"b_yuv444p16_2020ncl_pq": 1e-4, "b_ictcp_pq_half": 5e-4}
+
+
+def test_oracle_matches_reference_golden_butteraugli(oracle_lib):
+    """Butteraugli has no SSIM-style cancellation: the FP64 restatement matches the
+    reference's norms to 1e-5 relative and its distortion-map samples to 1e-4, on every
+    colour path except the two PQ ones, where the reference's own FP32 colour arithmetic
+    moves the norms by up to 4e-4 (bounds stated above; the next test shows the cause)."""
+    from tests.golden.cases import build_case
     checked = 0
-    for case in data["cases"]:
-        if case["metric"] != "butteraugli" or case["w"] * case["h"] > 600_000:
-            continue
+    for case in _butteraugli_cases():
         (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
         norms, dmap = oracle_lib.butteraugli(oracle_lib.convert(p1, ls1, cs1), oracle_lib.convert(p2, ls2, cs2),
                                              case["intensity"], case["qnorm"])
         ref = case["norms"]
+        tol = _FP32_COLOUR_SENSITIVE.get(case["name"], 1e-5)
+        for k in range(3):
+            assert abs(norms[k] - ref[k]) <= tol * max(abs(ref[k]), 1e-6), (case["name"], k, norms, ref)
+        if case["name"] not in _FP32_COLOUR_SENSITIVE:
+            idx = np.array(case["distmap_sample"]["index"])
+            val = np.array(case["distmap_sample"]["value"])
+            np.testing.assert_allclose(dmap.reshape(-1)[idx], val, rtol=1e-4, atol=1e-6)
+        checked += 1
+    assert checked >= 17
+
+
+def test_butteraugli_on_reference_colour_arithmetic_matches_every_path(oracle_lib):
+    """The FP64 Butteraugli fed with the reference's own float colour conversion
+    (ssimu2_f32.c's restatement of src/gpuColorToLinear) matches the reference's norms to
+    1e-5 on every colour path, PQ and ICtCp included: the PQ gaps above are the reference's
+    float colour arithmetic, not a difference in the metric."""
+    from tests.golden.cases import build_case
+    for case in _butteraugli_cases():
+        (p1, ls1, cs1), (p2, ls2, cs2) = build_case(case)
+        r1 = oracle_lib.convert_f32(p1, ls1, cs1).astype(np.float64)
+        r2 = oracle_lib.convert_f32(p2, ls2, cs2).astype(np.float64)
+        norms, _ = oracle_lib.butteraugli(r1, r2, case["intensity"], case["qnorm"])
+        ref = case["norms"]
         for k in range(3):
             assert abs(norms[k] - ref[k]) <= 1e-5 * max(abs(ref[k]), 1e-6), (case["name"], k, norms, ref)
-        idx = np.array(case["distmap_sample"]["index"])
-        val = np.array(case["distmap_sample"]["value"])
-        np.testing.assert_allclose(dmap.reshape(-1)[idx], val, rtol=1e-4, atol=1e-6)
-        checked += 1
-    assert checked >= 5
