@@ -62,7 +62,27 @@ def maps_flop_per_pair(w, h):
     return tiles * 1024 * 370
 
 
-FP32_NOMINAL_TFLOPS = 80.0  # B200 FP32 SIMT, nominal
+B200_SMS = 148
+FP32_LANES_PER_SM = 128
+
+
+def fp32_peak_tflops(clocks):
+    """FP32 SIMT peak at the SM clock sampled during the timed region: SMs x FP32 lanes x 2
+    FLOP per FMA x clock.  Falls back to the maximum SM clock (1965 MHz) without samples."""
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+    return round(B200_SMS * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12, 2), \
+        "%d SMs x %d FP32 lanes x 2 x %.0f MHz (sampled SM clock)" % (B200_SMS, FP32_LANES_PER_SM, mhz)
+
+
+def traffic_of(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.json),
+    with its provenance, or (None, None)."""
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(tp):
+        return None, None
+    with open(tp) as f:
+        tr = json.load(f).get(kernel)
+    return (tr.get("bytes_per_launch"), tr.get("source")) if tr else (None, None)
 
 
 def log(*a):
@@ -233,16 +253,12 @@ def run_ours(args, world, rank, local):
         # FP32 ridge): its compute fraction is the descriptive figure.
         flop = maps_flop_per_pair(W, H) * BATCH
         tf = flop / (avg_ms / 1e3) / 1e12
+        pk = fp32_peak_tflops(clocks)
         roofline["compute"] = {"flop_per_launch": flop, "achieved_tflops": round(tf, 2),
-                               "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_source": "nominal FP32 SIMT",
-                               "frac": round(tf / FP32_NOMINAL_TFLOPS, 4)}
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            tr = json.load(f).get(top_name)
-        if tr:
-            roofline["traffic"] = tr.get("bytes_per_launch")
-            roofline["traffic_source"] = tr.get("source")
+                               "peak_tflops": pk[0], "peak_source": pk[1], "frac": round(tf / pk[0], 4)}
+    roofline["traffic"], src = traffic_of(top_name)
+    if src:
+        roofline["traffic_source"] = src
 
     # ---------------- end to end through the C ABI (e2e) ----------------
     nthreads = args.e2e_threads
@@ -393,11 +409,186 @@ def run_reference(args, world, rank, local):
                    "api": "Vship_ComputeSSIMU2, each frame in one pinned buffer (FFVship layout)",
                    "threads_handlers": nthreads,
                    "threads_swept": args.ref_threads},
-        "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": input_bytes(pairs),
+                "d2h_bytes_per_step": BATCH * 4 * 108},
         "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "kind": "reference", "cores": nthreads,
                          "sample": "%d steps of %d pairs; the reference has no CPU implementation, so its own CUDA "
                                    "build runs on the B200, driven by %d host threads" % (args.steps, BATCH, nthreads)},
     }
+    print(json.dumps(line), flush=True)
+
+
+PWORKLOAD = "ssimu2_1080p_srgb8_single_pair"
+SCOPIES = 16  # distinct copies of the pair cycled through, 199 MB of input: larger than L2
+RGB8_BYTES_PER_IMAGE = 3 * W * H
+
+
+def single_pair(rank):
+    """One 1080p 8-bit sRGB pair (full range, BT.709 primaries) as the single-pair
+    configuration describes it: sinusoid-sum content + N(0, 3) noise, distorted by 8x8 DCT
+    quantisation with step 16."""
+    from vship_b200 import synth
+    return synth.make_pairs(1, W, H, fmt="rgb8", seed=4321 + rank, steps=16.0)[0]
+
+
+def single_e2e(api, cs, host_pairs, ls, local, threads_list, calls, warmup, lib=None):
+    """Through Vship_ComputeSSIMU2 (host frames): latency of one thread's sequential calls and
+    the best throughput over T threads with a handler each, every call scoring one pair of the
+    cycled copies.  Returns (latency_ms, best pairs/s, its thread count, {T: pairs/s})."""
+    import torch
+    sweep = {}
+    lat = None
+    for nthreads in threads_list:
+        handlers = [api.SSIMU2(cs, gpu_id=local, lib=lib) for _ in range(nthreads)]
+
+        def worker(k, n):
+            torch.cuda.set_device(local)
+            for i in range(n):
+                fr = host_pairs[(k * 7 + i) % len(host_pairs)]
+                handlers[k].compute(fr[0], fr[1], ls, ls)
+
+        def run(n):
+            ths = [threading.Thread(target=worker, args=(k, n)) for k in range(nthreads)]
+            for t in ths:
+                t.start()
+            for t in ths:
+                t.join()
+
+        run(warmup)
+        t0 = time.perf_counter()
+        run(calls)
+        dt = time.perf_counter() - t0
+        sweep[nthreads] = round(nthreads * calls / dt, 2)
+        if nthreads == 1:
+            lat = dt / calls * 1e3
+        for hh in handlers:
+            hh.close()
+    best_t = max(sweep, key=sweep.get)
+    return lat, sweep[best_t], best_t, sweep
+
+
+def run_single(args, rank, local, reference=False):
+    """Single-pair configuration: one 1080p 8-bit sRGB pair per call.  The reference's own
+    benchmark separates latency (sequential calls) from throughput (several threads and
+    handlers, test/apibenchmark.cpp:110-117); both are reported, for the device-resident entry
+    (ours only) and end to end through Vship_ComputeSSIMU2 with pinned host frames."""
+    import torch
+    from vship_b200 import abi, api
+    torch.cuda.set_device(local)
+    lib = None
+    if reference:
+        ref = os.path.join(ROOT, "oracle", "_ref", "libvship_ref.so")
+        if not os.path.exists(ref):
+            print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libvship_ref.so was not built"}))
+            return
+        lib = api.load_library(ref)
+    cs = abi.srgb8(W, H)
+    p1, p2, ls = single_pair(rank)
+    pairs = [(p1, p2, ls)] * SCOPIES
+    pinned, host_pairs = pinned_frames(pairs, api, lib=lib)
+    calls = max(args.steps, 1) * SCOPIES
+    threads = [1, 2, 3, 4, 8]
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    lat, e2e, e2e_t, sweep = single_e2e(api, cs, host_pairs, ls, local, threads, calls, args.warmup * SCOPIES, lib=lib)
+    clocks = sampler.stop()
+    for pb in pinned:
+        pb.free()
+    config = {"workload": PWORKLOAD, "pairs_per_call": 1, "width": W, "height": H, "format": "RGB 8-bit full range sRGB",
+              "distortion": "8x8 DCT quantisation, step 16",
+              "l2": "%d copies of the pair cycled (%.0f MB of input, larger than L2)" % (SCOPIES, SCOPIES * 2 * RGB8_BYTES_PER_IMAGE / 1e6)}
+    common = {"metric": "1080p SSIMU2 frame-pairs/s, single pair per call", "unit": UNIT, "n_gpus": 1,
+              "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+              "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+    e2e_obj = {"value": round(e2e, 2), "unit": UNIT, "api": "Vship_ComputeSSIMU2, each frame in one pinned buffer",
+               "threads_handlers": e2e_t, "threads_swept": sweep, "latency_ms": round(lat, 4),
+               "timer": "wall clock", "h2d_bytes_per_step": calls * 2 * RGB8_BYTES_PER_IMAGE,
+               "d2h_bytes_per_step": calls * 8}
+    if reference:
+        line = dict(common, impl="reference", value=round(e2e, 2), ms_per_step=round(calls / e2e * 1e3, 3),
+                    config=dict(config, library="Vship 4.1.0 built from its sources with nvcc for sm_100a "
+                                "(oracle/build_ref.sh)", calls_per_step=calls),
+                    e2e=e2e_obj, clocks=clocks,
+                    cpu_baseline={"value": round(e2e, 2), "unit": UNIT, "kind": "reference", "cores": e2e_t,
+                                  "sample": "%d calls per thread; the reference has no CPU implementation, so its "
+                                            "own CUDA build runs on the B200" % calls})
+        print(json.dumps(line), flush=True)
+        return
+
+    # device-resident: the pair copies in HBM, one pair per call on one stream
+    dev = [([torch.from_numpy(p).cuda() for p in p1], [torch.from_numpy(p).cuda() for p in p2]) for _ in range(SCOPIES)]
+    ptrs = [([t.data_ptr() for t in a], [t.data_ptr() for t in b]) for a, b in dev]
+    score = torch.zeros(1, dtype=torch.float64, device="cuda")
+    h = api.SSIMU2(cs, gpu_id=local)
+    stream = torch.cuda.current_stream()
+
+    def one(i):
+        a, b = ptrs[i % SCOPIES]
+        h.compute_device(1, a, b, ls, ls, score.data_ptr(), 0, stream.cuda_stream)
+
+    for i in range(args.warmup * SCOPIES):
+        one(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(calls):
+        one(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    value = calls / (ms / 1e3)
+    # per-call latency: host enqueue to completion of one call, calls one at a time
+    lats = []
+    for i in range(min(calls, 64)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one(i)
+        torch.cuda.synchronize()
+        lats.append((time.perf_counter() - t0) * 1e3)
+    h.kernel_timing(True)
+    h.kernel_times(reset=True)
+    for i in range(calls):
+        one(i)
+    torch.cuda.synchronize()
+    ktimes = h.kernel_times(reset=True)
+    h.kernel_timing(False)
+    got = float(score.item())
+    h.close()
+    top_name, (launches, total_ms) = max(ktimes.items(), key=lambda kv: kv[1][1])
+    avg_ms = total_ms / launches
+    peak, peak_kind = measured_peaks()
+    algo = {"ssimu2_front": 2 * (RGB8_BYTES_PER_IMAGE + 4 * XYB_FLOATS_PER_IMAGE), "ssimu2_maps": 2 * 4 * XYB_FLOATS_PER_IMAGE,
+            "ssimu2_final": 0}[top_name]
+    achieved = algo / (avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": top_name, "achieved": round(achieved, 1), "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(avg_ms, 4),
+                "kernels_ms_per_launch": {k: round(v[1] / v[0], 4) for k, v in ktimes.items()},
+                "note": "one pair per launch: the pyramid (33 MB) stays in L2 between the front and maps kernels"}
+    if top_name == "ssimu2_maps":
+        flop = maps_flop_per_pair(W, H)
+        tf = flop / (avg_ms / 1e3) / 1e12
+        pk = fp32_peak_tflops(clocks)
+        roofline["compute"] = {"flop_per_launch": flop, "achieved_tflops": round(tf, 2), "peak_tflops": pk[0],
+                               "peak_source": pk[1], "frac": round(tf / pk[0], 4)}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+        oracle.build()
+        t0, n = time.perf_counter(), 0
+        while n == 0 or (time.perf_counter() - t0) < min(args.cpu_seconds, 10.0):
+            _, exact, _ = oracle.ssimu2(oracle.convert(p1, ls, cs), oracle.convert(p2, ls, cs))
+            n += 1
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(n / dt, 3), "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+               "sample": "the pair scored %d times by the FP64 oracle (colour conversion + SSIMU2, %.1f s)" % (n, dt),
+               "max_abs_dscore_gpu_vs_fp64": abs(got - exact)}
+    line = dict(common, value=round(value, 2), ms_per_step=round(ms / max(args.steps, 1), 4),
+                config=dict(config, calls_per_step=SCOPIES),
+                latency_ms={"device_call_median": round(statistics.median(lats), 4),
+                            "device_stream_per_pair": round(ms / calls, 4), "e2e_sequential": round(lat, 4)},
+                e2e=e2e_obj, gpu_launches=3 * calls, roofline=roofline, cpu_baseline=cpu, clocks=clocks)
     print(json.dumps(line), flush=True)
 
 
@@ -435,14 +626,19 @@ def run_butteraugli(args, world, rank, local):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     value = BBATCH * args.steps / (ms / 1e3)
+    dev_norms = norms.cpu().numpy().copy()
     h.kernel_timing(True)
     h.kernel_times(reset=True)
     step()
@@ -454,6 +650,21 @@ def run_butteraugli(args, world, rank, local):
     e2e, e2e_threads, sweep = butter_e2e(args, pairs, cs, ls, local)
     peak, peak_kind = measured_peaks()
     achieved = B_ALGO_BYTES / (sum(v[1] for v in ktimes.values()) / BBATCH / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle
+        oracle.build()
+        k, t0, maxrel = 0, time.perf_counter(), 0.0
+        while k < BBATCH and (k == 0 or time.perf_counter() - t0 < args.cpu_seconds):
+            p1, p2, _ = pairs[k]
+            on, _ = oracle.butteraugli(oracle.convert(p1, ls, cs), oracle.convert(p2, ls, cs), 203.0, 5)
+            maxrel = max(maxrel, max(abs(dev_norms[k][j] - on[j]) / abs(on[j]) for j in range(3)))
+            k += 1
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(k / dt, 4), "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+               "sample": "first %d 4K pairs of the workload, colour conversion + Butteraugli in FP64 (%.1f s)" % (k, dt),
+               "max_rel_dnorm_gpu_vs_fp64": maxrel}
+    traffic, traffic_src = traffic_of("butteraugli_pair")
     line = {"metric": BMETRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -464,8 +675,11 @@ def run_butteraugli(args, world, rank, local):
                     "h2d_bytes_per_step": BBATCH * 2 * 3 * BW * BH, "d2h_bytes_per_step": BBATCH * (BW * BH * 4 + 24)},
             "kernels_ms_per_pair": per_pair_ms,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "peak_source": peak_kind,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                         "algorithmic_bytes_per_pair": B_ALGO_BYTES, "scope": "whole pipeline"}}
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "traffic_source": traffic_src, "algorithmic_bytes_per_pair": B_ALGO_BYTES,
+                         "scope": "whole pipeline, per pair"},
+            "gpu_launches": args.steps * sum(v[0] for v in ktimes.values()),
+            "cpu_baseline": cpu, "clocks": clocks}
     print(json.dumps(line), flush=True)
 
 
@@ -572,8 +786,6 @@ def run_cvvdp(args, rank, local, reference=False):
         line["impl"] = "reference"
         line["cpu_baseline"] = {"value": round(fps, 2), "unit": "frames/s", "kind": "reference", "cores": nthreads,
                                 "sample": "the reference has no CPU implementation: its own CUDA build on the B200"}
-        line["e2e"]["h2d_bytes_per_step"] = 0
-        line["e2e"]["d2h_bytes_per_step"] = 0
     print(json.dumps(line), flush=True)
 
 
@@ -638,7 +850,8 @@ def run_butteraugli_reference(args, rank, local):
                        "library": "Vship 4.1.0 built from its sources with nvcc for sm_100a (oracle/build_ref.sh)",
                        "api": "Vship_ComputeButteraugli with distortion map, pinned frames",
                        "threads_handlers": nthreads, "threads_swept": sweep},
-            "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": BBATCH * 2 * 3 * BW * BH,
+                    "d2h_bytes_per_step": BBATCH * (BW * BH * 4 + 4)},
             "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "kind": "reference", "cores": nthreads,
                              "sample": "the reference has no CPU implementation: its own CUDA build on the B200"}}
     print(json.dumps(line), flush=True)
@@ -852,9 +1065,13 @@ def run_uneven(args, world, rank, local):
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "kernel": "ssimu2_batch", "achieved": round(achieved, 1), "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                     "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(avg_ms, 4)},
+                     "algorithmic_bytes_per_launch": algo, "avg_launch_ms": round(avg_ms, 4),
+                     "scope": "the whole graph launch (front, tile table, maps, final)"},
         "cpu_baseline": cpu, "clocks": clocks,
     }
+    tr, src = traffic_of("ssimu2_batch")
+    if tr:
+        line["roofline"]["traffic"], line["roofline"]["traffic_source"] = tr, src
     print(json.dumps(line), flush=True)
 
 
@@ -916,7 +1133,9 @@ def run_uneven_reference(args, world, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": UWORKLOAD, "pairs_per_step": n, "threads_handlers": nthreads,
                    "api": "Vship_ComputeSSIMU2 per pair, one handler per resolution per thread"},
-        "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(v, 2), "unit": UNIT,
+                "h2d_bytes_per_step": sum(p.nbytes for _, a, b, _ in pairs for p in list(a) + list(b)),
+                "d2h_bytes_per_step": n * 4 * 108},
         "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "kind": "reference", "cores": nthreads,
                          "sample": "the reference's CUDA build on the B200 driven by %d host threads" % nthreads}}),
         flush=True)
@@ -1164,8 +1383,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cvvdp-threads", type=int, nargs="+", default=[1, 2, 4],
                     help="cvvdp: concurrent sequences (handlers) swept")
-    ap.add_argument("--metric", default="ssimu2", choices=["ssimu2", "butteraugli", "ssimu2-uneven", "surrogate", "cvvdp"],
-                    help="butteraugli: secondary 4K Butteraugli line; ssimu2-uneven: 256 pairs of mixed "
+    ap.add_argument("--metric", default="ssimu2",
+                    choices=["ssimu2", "ssimu2-single", "butteraugli", "ssimu2-uneven", "surrogate", "cvvdp"],
+                    help="ssimu2-single: one 1080p 8-bit sRGB pair per call (latency and throughput); "
+                         "butteraugli: secondary 4K Butteraugli line; ssimu2-uneven: 256 pairs of mixed "
                          "resolutions in one persistent launch, instead of the headline metric")
     ap.add_argument("--tile-rows", type=int, default=0, help="ssimu2-uneven: fixed map tile rows (0: autotune)")
     ap.add_argument("--sur-train", type=int, default=200000, help="surrogate: training pairs")
@@ -1206,6 +1427,10 @@ def main():
     if args.metric == "cvvdp":
         if rank == 0:
             run_cvvdp(args, rank, local, reference=args.impl == "reference")
+        return
+    if args.metric == "ssimu2-single":
+        if rank == 0:
+            run_single(args, rank, local, reference=args.impl == "reference")
         return
     if args.metric == "surrogate":
         if args.impl == "reference":
