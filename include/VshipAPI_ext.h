@@ -55,10 +55,11 @@ EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliKernelTiming(Vship_Butterau
 EXPORTPREPROCESS int VshipExt_ButteraugliKernelTimes(Vship_ButteraugliHandler handler, VshipExt_KernelTime* out, int max, int reset);
 
 /* Scores one frame pair already in device memory without allocating anything, for callers
- * that cannot call cudaMalloc: work being recorded into a CUDA graph by stream capture, a
- * process whose GPU memory is handed out up front by a fixed budget or pool, or a real-time
- * loop that must never enter the driver's allocator.  This function has no counterpart in the
- * reference library.
+ * that cannot call cudaMalloc: a process whose GPU memory is handed out up front by a fixed
+ * budget or pool (an allocation outside it fails or takes memory another component was
+ * promised), or a real-time loop that must never enter the driver's allocator (a cudaMalloc
+ * can block for milliseconds and synchronise the device).  This function has no counterpart
+ * in the reference library.
  *
  * It runs on the current device, with no handler: the colourspaces are passed directly
  * (resize and crop are not supported here; use a handler for those).  Inputs are three device
@@ -74,7 +75,9 @@ EXPORTPREPROCESS int VshipExt_ButteraugliKernelTimes(Vship_ButteraugliHandler ha
  * call before any stream capture.  Every call shares the one array per device: calls whose
  * work overlaps on the GPU (different streams, or host threads without ordering) race and
  * corrupt each other's results; serialise them.  Each call writes every scratch byte it
- * reads, so nothing left by a previous call leaks into a result. */
+ * reads, so nothing left by a previous call leaks into a result.  The device address and the
+ * blur constants are cached per device for the life of the process: after cudaDeviceReset do
+ * not call this entry point on that device again. */
 EXPORTPREPROCESS Vship_Exception VshipExt_ComputeSSIMU2NoAlloc(Vship_Colorspace_t src_colorspace,
                                                                 Vship_Colorspace_t dis_colorspace, double* d_score,
                                                                 float* d_features, const uint8_t* const srcp1[3],

@@ -8,7 +8,10 @@ are carried over as data: each decimal literal is rounded the way the reference'
 rounds it (to double, then to the float array element) and written as an exact hexadecimal
 float literal.
 
-Usage: python cvvdp_csf_table.py [path/to/csf_lut_weber.hpp]
+Test tooling: it reads the reference's sources and writes the library's header
+vship_b200/csrc/cvvdp_csf_table.h; nothing in the library runs it.
+
+Usage: python -m tests.golden.cvvdp_csf_table [path/to/csf_lut_weber.hpp]
 (default: $VSHIP_REFERENCE_ROOT/src/cvvdp/csf_lut_weber.hpp, VSHIP_REFERENCE_ROOT defaulting
 to /root/reference).  tests/test_cvvdp_oracle.py regenerates the header from the same file,
 when it is present, and checks that the committed one is identical.
@@ -19,7 +22,8 @@ import struct
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-OUT = os.path.join(HERE, "cvvdp_csf_table.h")
+ROOT = os.path.dirname(os.path.dirname(HERE))
+OUT = os.path.join(ROOT, "vship_b200", "csrc", "cvvdp_csf_table.h")
 
 
 def default_source():

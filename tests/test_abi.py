@@ -142,3 +142,22 @@ int main(void){
     assert vals == [ctypes.sizeof(abi.Colorspace), abi.Colorspace.sample.offset, abi.Colorspace.crop.offset,
                     ctypes.sizeof(abi.DeviceInfo), ctypes.sizeof(abi.ButteraugliScore), ctypes.sizeof(abi.Version),
                     ctypes.sizeof(abi.FramePair), abi.FramePair.srcp1.offset, abi.FramePair.lineSize2.offset]
+
+
+def test_ssimu2_weights_match_reference_source():
+    """The 108 SSIMULACRA2 weights the engine, the oracle and the tests share
+    (vship_b200/csrc/metric_tables.h) are the reference's own float array
+    (src/ssimu2/score.hpp:5-113), compared value for value after rounding both to float."""
+    import numpy as np
+    from tests import tables
+    src = os.path.join(os.environ.get("VSHIP_REFERENCE_ROOT", "/root/reference"), "src", "ssimu2", "score.hpp")
+    if not os.path.exists(src):
+        pytest.skip("reference sources not present")
+    text = open(src).read()
+    body = text[text.index("weights[108]"):]
+    body = body[body.index("{") + 1:body.index("}")]
+    ref = np.array([float(v) for v in re.findall(r"-?\d+(?:\.\d*)?(?:[eE][-+]?\d+)?", body)], dtype=np.float32)
+    assert ref.size == 108
+    np.testing.assert_array_equal(tables.weights().astype(np.float32), ref)
+    prune = float(re.search(r"weight_pruning\s*=\s*([0-9.]+)f", text).group(1))
+    assert np.float32(prune) == np.float32(0.01)

@@ -33,11 +33,7 @@ JOD_TOL = 2e-4
 
 
 def test_csf_table_matches_reference_source():
-    sys.path.insert(0, os.path.join(ROOT, "vship_b200", "csrc"))
-    try:
-        import cvvdp_csf_table as gen
-    finally:
-        sys.path.pop(0)
+    from tests.golden import cvvdp_csf_table as gen
     src = gen.default_source()
     if not os.path.exists(src):
         pytest.skip("reference sources not present")

@@ -135,3 +135,41 @@ def test_contiguous_frame_single_copy_matches_separate_planes(gpu):
         got, _ = hb.compute([buf1.ctypes.data + int(o[i]) for i in range(3)],
                             [buf2.ctypes.data + int(o[i]) for i in range(3)], pls)
         assert got == sep
+
+
+def _odd_device_planes(planes):
+    """Each plane copied to device memory one byte past an even address: strides stay even
+    but every plane pointer is odd."""
+    import torch
+    out, keep = [], []
+    for p in planes:
+        raw = np.ascontiguousarray(p).view(np.uint8).reshape(-1)
+        buf = torch.zeros(raw.size + 16, dtype=torch.uint8, device="cuda")
+        buf[1:1 + raw.size] = torch.from_numpy(raw).cuda()
+        keep.append(buf)
+        out.append(buf.data_ptr() + 1)
+    return out, keep
+
+
+def test_device_path_with_odd_plane_addresses(gpu):
+    """16-bit samples at odd device addresses (even strides) take byte loads and score exactly
+    as the host path, which stages the frames at aligned addresses."""
+    import torch
+    w, h = 130, 98
+    p1, p2, ls = synth.make_pairs(1, w, h, fmt="yuv420p10", seed=31)[0]
+    cs = abi.yuv420_10bit_bt709(w, h)
+    a, ka = _odd_device_planes(p1)
+    b, kb = _odd_device_planes(p2)
+    assert all(x % 2 == 1 for x in a + b)
+    score = torch.zeros(1, dtype=torch.float64, device="cuda")
+    with api.SSIMU2(cs) as hd:
+        want = hd.compute(p1, p2, ls)
+        hd.compute_device(1, a, b, ls, ls, score.data_ptr(), 0, 0)
+        torch.cuda.synchronize()
+    assert score.item() == want, (score.item(), want)
+    norms = torch.zeros(3, dtype=torch.float64, device="cuda")
+    with api.Butteraugli(cs, qnorm=5, intensity=203.0) as hb:
+        bwant, _ = hb.compute(p1, p2, ls)
+        hb.compute_device(a, b, ls, ls, norms.data_ptr())
+        torch.cuda.synchronize()
+    assert tuple(norms.cpu().numpy()) == tuple(bwant), (norms.cpu().numpy(), bwant)

@@ -157,6 +157,9 @@ Vship_Exception with_handler(Table<EngineT>& table, unsigned id, const char* whe
     try {
         CUDA_CHECK(cudaSetDevice(s->gpu));
         fn(*s);
+#ifdef VSHIP_BOUNDS_CHECK
+        check_guards(where);
+#endif
     } catch (const Error& e) {
         rc = fail(s, e);
     } catch (const std::bad_alloc&) {
@@ -178,6 +181,26 @@ int device_count_or_throw() {
     return count;
 }
 
+#ifdef VSHIP_BOUNDS_CHECK
+constexpr size_t kGuardBytes = 64u << 10;
+
+struct GuardedBlock {
+    unsigned char* base;   // start of the lower guard band
+    size_t bytes;          // payload bytes
+    std::string what;
+    int device;
+};
+
+std::mutex g_guard_lock;
+std::vector<GuardedBlock> g_guarded;
+unsigned* g_guard_flag[64] = {};
+
+__global__ void guard_check_kernel(const unsigned char* lo, const unsigned char* hi, size_t n, unsigned* bad) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (lo[i] != 0xFFu || hi[i] != 0xFFu) atomicOr(bad, 1u);
+}
+#endif
+
 __global__ void kernel_test(int* out) { out[0] = 4320984; }
 
 // One-thread sanity kernel (src/util/gpuhelper.hpp:40-54).
@@ -196,6 +219,57 @@ bool kernel_check() {
     }
     return host == 4320984;
 }
+
+#ifdef VSHIP_BOUNDS_CHECK
+}  // namespace
+
+void* guarded_alloc(size_t bytes, const char* what) {
+    unsigned char* p = nullptr;
+    if (cudaMalloc(&p, bytes + 2 * kGuardBytes) != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw Error(Vship_OutOfVRAM, __FILE__, __LINE__, std::string("cudaMalloc failed for ") + what);
+    }
+    CUDA_CHECK(cudaMemset(p, 0xFF, bytes + 2 * kGuardBytes));
+    int dev = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(g_guard_lock);
+    g_guarded.push_back(GuardedBlock{p, bytes, what, dev});
+    return p + kGuardBytes;
+}
+
+void guarded_free(void* user) {
+    if (!user) return;
+    std::lock_guard<std::mutex> g(g_guard_lock);
+    for (size_t i = 0; i < g_guarded.size(); i++)
+        if (g_guarded[i].base + kGuardBytes == user) {
+            (void)cudaFree(g_guarded[i].base);
+            g_guarded.erase(g_guarded.begin() + (long)i);
+            return;
+        }
+}
+
+void check_guards(const char* where) {
+    CUDA_CHECK(cudaDeviceSynchronize());
+    int dev = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(g_guard_lock);
+    if (dev < 0 || dev >= 64) return;
+    if (!g_guard_flag[dev]) CUDA_CHECK(cudaMalloc(&g_guard_flag[dev], sizeof(unsigned)));
+    for (const GuardedBlock& b : g_guarded) {
+        if (b.device != dev) continue;
+        CUDA_CHECK(cudaMemset(g_guard_flag[dev], 0, sizeof(unsigned)));
+        guard_check_kernel<<<64, 256>>>(b.base, b.base + kGuardBytes + b.bytes, kGuardBytes, g_guard_flag[dev]);
+        CUDA_CHECK(cudaGetLastError());
+        unsigned bad = 0;
+        CUDA_CHECK(cudaMemcpy(&bad, g_guard_flag[dev], sizeof(unsigned), cudaMemcpyDeviceToHost));
+        if (bad)
+            throw Error(Vship_HIPError, __FILE__, __LINE__,
+                        std::string("a kernel wrote past the bounds of ") + b.what + " (found after " + where + ")");
+    }
+}
+
+namespace {
+#endif
 
 template <typename EngineT, typename InitFn>
 Vship_Exception init_handler(Table<EngineT>& table, unsigned* id_out, int gpu, InitFn init) {
@@ -866,5 +940,27 @@ Vship_Exception VshipExt_SurrogateKernelTiming(VshipExt_SurrogateHandler handler
 int VshipExt_SurrogateKernelTimes(VshipExt_SurrogateHandler handler, VshipExt_KernelTime* out, int max, int reset) {
     return kernel_times(g_surrogate, handler.id, out, max, reset);
 }
+
+#ifdef VSHIP_BOUNDS_CHECK
+// Bounds-check build only: checks the guard-band checker itself on the current device.  It
+// allocates a guarded 1 KiB buffer and, when `corrupt` is non-zero, changes one byte of its
+// upper guard band from the host (cudaMemset inside the allocation: no kernel steps out of
+// bounds), then runs the guard check.  Returns its code: Vship_NoError for an intact band,
+// Vship_HIPError when the change was found.
+__attribute__((visibility("default"))) Vship_Exception VshipExt_BoundsCheckProbe(int corrupt) {
+    unsigned char* p = nullptr;
+    Vship_Exception rc = Vship_NoError;
+    try {
+        p = static_cast<unsigned char*>(guarded_alloc(1024, "the probe buffer"));
+        if (corrupt) CUDA_CHECK(cudaMemset(p + 1024 + 100, 0x00, 1));
+        check_guards("VshipExt_BoundsCheckProbe");
+    } catch (const Error& e) {
+        set_global_error(e);
+        rc = e.code;
+    }
+    guarded_free(p);
+    return rc;
+}
+#endif
 
 }  // extern "C"

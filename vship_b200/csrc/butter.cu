@@ -773,10 +773,10 @@ public:
             for (int p = 0; p < 3; p++) {
                 if (src[p] == nullptr) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
                 if (ls[p] < geo_[c].pw[p] * geo_[c].bytes) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
-                if (ls[p] % geo_[c].bytes) cp[c].misaligned = 1;
                 raw[c].p[p] = src[p];
                 raw[c].stride[p] = ls[p];
             }
+            if (misaligned_view(raw[c], geo_[c])) cp[c].misaligned = 1;
         }
         if (d_distmap && (dststride % 4 || dststride < (int64_t)w_ * 4))
             VSHIP_THROW(Vship_BadPointer, "distmap stride must be a multiple of 4 bytes and at least width * 4");

@@ -510,9 +510,48 @@ __device__ __forceinline__ float2 chroma_from_stage(const ChromaStage& st, const
     return make_float2(out[0], out[1]);
 }
 
+// ICtCp (BT.2100) to linear RGB in FP64: I'Ct'Cp' -> L'M'S' (YUVToLinRGB.hpp:47-63), the
+// transfer, LMS -> RGB (:28-43), with the reference's sequential substitutions.  Both
+// matrices subtract nearly equal terms (S' = 33.03 L' - 32.03 M' - 7.54 Cp, R = 3.44 L -
+// 2.51 M + ...), and PQ raises (V^(1/m) - c1) to 1/n ~ 6.3, so FP32 rounding anywhere in
+// this chain reaches ~1e-4 of the linear value of dark pixels and moves Butteraugli norms by
+// a few 1e-4.  Only ICtCp clips take this path.
+static __device__ __noinline__ float3 ictcp_to_linear(float3 in, int trc) {
+    const double I = in.x, Ct = in.y, Cp = in.z;
+    double v[3];
+    v[0] = fma(Ct, 0.0086090370379327566, fma(Cp, 0.11102962500302595655, I));
+    v[1] = fma(Ct, -0.01721807407586551, fma(Cp, -0.22205925000605192, v[0]));
+    v[2] = fma(v[0], 33.025782688766114, fma(v[1], -32.025782688766114, -Cp * 7.543278084714549));
+    if (trc == Vship_TRC_PQ) {
+        const double m = 78.843750000000000, n = 0.15930175781250000;
+        const double c1 = 0.83593750000000000, c2 = 18.851562500000000, c3 = 18.687500000000000;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const double x = pow(fmax(0.0, v[k]), 1.0 / m);
+            v[k] = 100.0 * pow(fmax(0.0, x - c1) / (c2 - c3 * x), 1.0 / n);
+        }
+    } else if (trc == Vship_TRC_HLG) {
+        const double a = 0.17883277, b = 1.0 - 4.0 * a, c = 0.5 - a * -0.3350097945111627;
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = v[k] <= 0.5 ? v[k] * v[k] / 3.0 : (exp((v[k] - c) / a) + b) / 12.0;
+        const double s = pow(0.2627 * v[0] + 0.6780 * v[1] + 0.0593 * v[2], 1.2 - 1.0);
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] *= s;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = (double)trc_one((float)v[k], trc);
+    }
+    const double L = v[0], M = v[1], S = v[2];
+    const double R = fma(L, 3.4366066943330784267, fma(M, -2.5064521186562698975, S * 0.069845424323191470954));
+    const double G = fma(R, -0.23026480071281397, fma(M, 1.4064527541936944, -S * 0.2083538389058436));
+    const double B = fma(R, -0.02684381778741865, fma(G, -0.08378524945770065, S * 1.106879231557486));
+    return make_float3((float)R, (float)G, (float)B);
+}
+
 // Y'CbCr (or R'G'B') -> linear RGB of one pixel in the clip's own primaries (the
 // reference's linRGB destination, src/gpuColorToLinear/vshipColor.hpp:111-113).
 __device__ __forceinline__ float3 to_linear_native(float3 v, const ColourParams& cp) {
+    if (cp.matrix == Vship_MATRIX_BT2100_ICTCP && !cp.skip_yuv) return ictcp_to_linear(v, cp.trc);
     if (!cp.skip_yuv) {
         v = gamma_light(v, cp.matrix);
         v = transfer(v, cp.trc);

@@ -47,9 +47,25 @@ struct Error {
         }                                                                                   \
     } while (0)
 
+#ifdef VSHIP_BOUNDS_CHECK
+// Bounds-check build (the stand-in for compute-sanitizer, which is not available on the GPU
+// pool): every device buffer the engines allocate gets a 64 KiB guard band on each side, and
+// the buffer and its guards start filled with 0xFF bytes (a NaN in every float and double).
+// A kernel that writes past either end of a buffer leaves a guard byte changed, which
+// check_guards() finds after each API call and reports as Vship_HIPError; a kernel that reads
+// past an end, or reads a float it never wrote, carries a NaN into the scores.  Defined in
+// api.cu.
+void* guarded_alloc(size_t bytes, const char* what);
+void guarded_free(void* p);
+void check_guards(const char* where);
+#endif
+
 // Device allocation that reports OutOfVRAM like the reference (src/ssimu2/main.hpp:127-133).
 template <typename T>
 inline T* device_alloc(size_t count, const char* what) {
+#ifdef VSHIP_BOUNDS_CHECK
+    return static_cast<T*>(guarded_alloc((count ? count : 1) * sizeof(T), what));
+#endif
     void* p = nullptr;
     if (count == 0) count = 1;
     cudaError_t e = cudaMalloc(&p, count * sizeof(T));
@@ -73,6 +89,10 @@ inline T* pinned_alloc(size_t count, const char* what) {
 }
 
 inline void device_free(void* p) {
+#ifdef VSHIP_BOUNDS_CHECK
+    guarded_free(p);
+    return;
+#endif
     if (p) (void)cudaFree(p);
 }
 

@@ -196,12 +196,15 @@ inline RawImage stage_host_image(StagingBuffer& buf, const ClipGeometry& g, cons
     return copy_host_image(buf.ptr, g, src, line_size, stream);
 }
 
-// A stride that is not a multiple of the sample size makes the kernels use byte loads.
-inline bool misaligned_view(const RawImage& im, const ClipGeometry& g) {
+// A stride or a plane address that is not a multiple of the sample size makes the kernels
+// use byte loads.
+inline bool misaligned_planes(const uint8_t* const p[3], const int64_t stride[3], int bytes) {
     for (int c = 0; c < 3; c++)
-        if (im.stride[c] % g.bytes || (reinterpret_cast<uintptr_t>(im.p[c]) % g.bytes)) return true;
+        if (stride[c] % bytes || (reinterpret_cast<uintptr_t>(p[c]) % bytes)) return true;
     return false;
 }
+
+inline bool misaligned_view(const RawImage& im, const ClipGeometry& g) { return misaligned_planes(im.p, im.stride, g.bytes); }
 
 // ---- generic path: ingest to planar linear RGB, then resize (horizontalResizeTranspose,
 // ---- src/gpuColorToLinear/resize.hpp:26-48), crop by offset.

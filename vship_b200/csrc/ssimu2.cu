@@ -284,10 +284,13 @@ public:
         ColourParams cp[2] = {cp_[0], cp_[1]};
         for (int c = 0; c < 2; c++) {
             const int64_t* ls = c ? ls2 : ls1;
-            for (int p = 0; p < 3; p++) {
+            const uint8_t* const* src = c ? d2 : d1;
+            for (int p = 0; p < 3; p++)
                 if (ls[p] < geo_[c].pw[p] * geo_[c].bytes) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
-                if (ls[p] % geo_[c].bytes) cp[c].misaligned = 1;
-            }
+            // the colour parameters are shared by the launch: one unaligned plane of any pair
+            // (stride or address) switches that clip to byte loads
+            for (int i = 0; i < n && !cp[c].misaligned; i++)
+                if (misaligned_planes(src + 3 * i, ls, geo_[c].bytes)) cp[c].misaligned = 1;
         }
         cudaStream_t st = stream;  // NULL: the CUDA legacy default stream
         CUDA_CHECK(cudaStreamWaitEvent(st, last_done_, 0));
@@ -472,9 +475,10 @@ private:
 // ------------------------------------------------------------------------------------------
 // Allocation-free scoring (VshipExt_ComputeSSIMU2NoAlloc)
 //
-// Some callers cannot call cudaMalloc: code recording or replaying work inside a stream
-// capture, a process whose GPU memory is handed out up front by a fixed budget or pool, or a
-// real-time loop that must not reach the driver's allocator.  For them this entry point
+// Some callers cannot call cudaMalloc: a process whose GPU memory is handed out up front by a
+// fixed budget or pool (an allocation outside it fails or steals from another component), or
+// a real-time loop that must not reach the driver's allocator, whose calls can block for
+// milliseconds and synchronise the device.  For them this entry point
 // scores one pair already in device memory with the same three kernels as the handler path,
 // but with all of its scratch -- both XYB pyramids, the tile partials and the map work list
 // -- in the file-scope array below.  The array is part of the library image: every GPU that
@@ -490,7 +494,9 @@ static unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
 
 // Device address of the scratch array on the current device.  The first call on a device
 // resolves it with cudaGetSymbolAddress (the host-side name is only a stand-in for the
-// device array) and loads the blur constants; later calls reuse the cached address.
+// device array) and loads the blur constants; later calls reuse the cached address.  The
+// cache lives as long as the process: after cudaDeviceReset the address and the constants
+// belong to a destroyed context, so the entry point must not be used on that device again.
 static unsigned char* noalloc_scratch_for_current_device() {
     int dev = -1;
     CUDA_CHECK(cudaGetDevice(&dev));
@@ -529,13 +535,11 @@ static void compute_no_alloc(const Vship_Colorspace_t& src, const Vship_Colorspa
     for (int c = 0; c < 2; c++) {
         const int64_t* ls = c ? ls2 : ls1;
         const uint8_t* const* d = c ? d2 : d1;
-        bool mis = false;
         for (int p = 0; p < 3; p++) {
             if (d[p] == nullptr) VSHIP_THROW(Vship_BadPointer, "null plane pointer");
             if (ls[p] < geo[c].pw[p] * geo[c].bytes) VSHIP_THROW(Vship_BadPointer, "lineSize smaller than one row of samples");
-            if (ls[p] % geo[c].bytes) mis = true;
         }
-        cp[c] = make_colour_params(*cs[c], geo[c], mis);
+        cp[c] = make_colour_params(*cs[c], geo[c], misaligned_planes(d, ls, geo[c].bytes));
     }
 
     // Pyramid layout, tile count and work list of one pair, as the handler path builds them.
@@ -643,6 +647,14 @@ extern "C" Vship_Exception VshipExt_ComputeSSIMU2NoAlloc(Vship_Colorspace_t src_
         vship::ssimu2::compute_no_alloc(src_colorspace, dis_colorspace, d_score, d_features, srcp1, srcp2, lineSize, lineSize2,
                                         (cudaStream_t)stream);
     } catch (const vship::Error& e) {
+        vship::record_global_error(e);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        vship::Error e(Vship_OutOfRAM, __FILE__, __LINE__, "VshipExt_ComputeSSIMU2NoAlloc");
+        vship::record_global_error(e);
+        return e.code;
+    } catch (const std::exception& ex) {
+        vship::Error e(Vship_BadErrorType, __FILE__, __LINE__, ex.what());
         vship::record_global_error(e);
         return e.code;
     }
