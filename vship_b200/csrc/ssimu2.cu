@@ -118,16 +118,16 @@ __global__ void __launch_bounds__(kMapThreads) ssimu2_maps_kernel(const __grid_c
     int tile = blockIdx.x;
     if (tile >= total_tiles) return;
     TileRef cur = locate_tile(mt, tile);
-    MT::Regs regs;
-    load_halo<kTile, false, true>(cur, regs);
+    HaloV4 regs;
+    load_halo_v4(cur, regs);
 
     while (true) {
-        stage_halo<kTile, true>(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
+        stage_halo_v4(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
         const int X0 = cur.X0, Y0 = cur.Y0, w = cur.w, h = cur.h;
         const int next = tile + gridDim.x;
         if (next < total_tiles) {
             cur = locate_tile(mt, next);
-            load_halo<kTile, false, true>(cur, regs);
+            load_halo_v4(cur, regs);
         }
         blur_score_tile<kTile>(sm, X0, Y0, w, h, partials + (int64_t)tile * 6);
         if (next >= total_tiles) break;

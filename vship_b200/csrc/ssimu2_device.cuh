@@ -349,6 +349,69 @@ __device__ __forceinline__ void stage_halo(typename MapTile<TH>::Smem& sm, const
     __syncthreads();
 }
 
+// Halo of a 32 x 32 map tile read with 128-bit loads (per-handler and no-allocation maps
+// kernels).  The halo is 48 rows of 12 float4 per image: halo column 0 is X0 - 8, a multiple
+// of 8, and plane rows are padded to a multiple of 8 floats, so every float4 starts on a
+// 16-byte boundary and a float4 that starts inside a row ends inside the row's padding.  A
+// float4 that starts left of the plane or in a row outside it is not read; elements at or
+// past the plane width are zeroed at staging (the padding holds no pixel).  Thread t holds
+// positions t + 128 i (i < 5; the fifth only for t < 64) of both images: 10 loads per tile
+// instead of 36 scalar ones.  The batch kernel, at its register limit, keeps load_halo.
+struct HaloV4 {
+    static constexpr int kRows = kTile + 2 * kHalo;
+    static constexpr int kVec = kIn / 4;
+    static constexpr int kPos = kRows * kVec;
+    static constexpr int kSlots = (kPos + kMapThreads - 1) / kMapThreads;
+    float4 a[kSlots], b[kSlots];
+    float ka, kb;
+    unsigned inmask;
+};
+
+__device__ __forceinline__ void load_halo_v4(const TileRef& t, HaloV4& r) {
+    const int64_t o0 = (int64_t)t.Y0 * t.pitch + t.X0;
+    r.ka = __ldg(t.a + o0);
+    r.kb = __ldg(t.b + o0);
+    r.inmask = 0;
+#pragma unroll
+    for (int it = 0; it < HaloV4::kSlots; it++) {
+        const int j = threadIdx.x + it * kMapThreads;
+        const int row = j / HaloV4::kVec, c4 = j - row * HaloV4::kVec;
+        const int gx = t.X0 - kHalo + 4 * c4, gy = t.Y0 - kHalo + row;
+        const bool in = j < HaloV4::kPos && (unsigned)gx < (unsigned)t.w && (unsigned)gy < (unsigned)t.h;
+        const int64_t o = in ? (int64_t)gy * t.pitch + gx : 0;
+        r.a[it] = in ? __ldg(reinterpret_cast<const float4*>(t.a + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        r.b[it] = in ? __ldg(reinterpret_cast<const float4*>(t.b + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        r.inmask |= (in ? 1u : 0u) << it;
+    }
+}
+
+// stage_halo for a HaloV4: the same shift, renormalisation tables and zero padding.
+__device__ __forceinline__ void stage_halo_v4(typename MapTile<kTile>::Smem& sm, const HaloV4& r, int X0, int Y0, int w,
+                                              int h) {
+    const int tid = threadIdx.x;
+    if (tid < kTile)
+        sm.invx[tid] = 1.0f / blur_norm(min(X0 + tid, w - 1), w);
+    else if (tid < 2 * kTile)
+        sm.invy[tid - kTile] = 1.0f / blur_norm(min(Y0 + tid - kTile, h - 1), h);
+    const float k = 0.5f * (r.ka + r.kb);
+#pragma unroll
+    for (int it = 0; it < HaloV4::kSlots; it++) {
+        const int j = tid + it * kMapThreads;
+        if (j >= HaloV4::kPos) break;
+        const int row = j / HaloV4::kVec, c4 = j - row * HaloV4::kVec;
+        const int gx = X0 - kHalo + 4 * c4;
+        const bool in = (r.inmask >> it) & 1u;
+        const float av[4] = {r.a[it].x, r.a[it].y, r.a[it].z, r.a[it].w};
+        const float bv[4] = {r.b[it].x, r.b[it].y, r.b[it].z, r.b[it].w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const bool ine = in && gx + e < w;
+            sm.sab[row][4 * c4 + e] = ine ? f2(av[e] - k, bv[e] - k) : f2(0.f, 0.f);
+        }
+    }
+    __syncthreads();
+}
+
 // Blurs a staged tile and scores it: separable 17-tap blur of the four moment inputs,
 // SSIM / artifact / detail-loss maps, and the tile's FP64 sums of x and x^4 of each map,
 // written by threads 0-5 to out[0..5].  Ends with the reduction barrier; the caller must
