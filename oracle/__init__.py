@@ -110,9 +110,7 @@ def lib():
         L.oracle_f32_convert.restype = ctypes.c_int
         L.oracle_f32_ssimu2.argtypes = [fp, fp, ctypes.c_int64, ctypes.c_int64, fp]
         L.oracle_f32_ssimu2.restype = ctypes.c_double
-        L.oracle_f32_set_variant.argtypes = [ctypes.c_int]
         L.oracle_f32_set_math.argtypes = [_MATH_FN]
-        L.oracle_f32_get_variant.restype = ctypes.c_int
         L.oracle_convert_native.argtypes = L.oracle_convert.argtypes
         L.oracle_convert_native.restype = ctypes.c_int
         vp, i64 = ctypes.c_void_p, ctypes.c_int64

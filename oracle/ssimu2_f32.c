@@ -31,29 +31,13 @@
 
 #define ORACLE_API __attribute__((visibility("default")))
 
-/* Contraction choices that the reference's source leaves to the compiler (bit set = the
- * product is fused into the following addition).  Settled against the reference's outputs;
- * the default is the set that reproduces them. */
-enum {
-    F32_HERMITE_HORNER = 1 << 0,   /* CubicHermitSplineInterpolator::get (resize.hpp:14-23)   */
-    F32_HERMITE_V2 = 1 << 1,       /* v2 = -3*p0 + 3*p1 ... (resize.hpp:10)                    */
-    F32_YUV_NUM = 1 << 2,          /* val.z + val.x*vscale (YUVToLinRGB.hpp:13-15)             */
-    F32_YUV_DEN = 1 << 3,          /* vscale*Kr + 0.5f, folded as one fused operation         */
-    F32_MAP_FMA = 1 << 4,          /* s12 - m1*m2 and the denominator (score.hpp:262-268)      */
-    F32_PQ_FMA = 1 << 5,           /* c2 - c3*a (transferToLinear.hpp:181)                      */
-    F32_HLG_FMA = 1 << 6,          /* Ys (transferToLinear.hpp:49)                              */
-    F32_HERMITE_V2_ALT = 1 << 7,   /* v2 with the 3*p1 product fused instead of -3*p0          */
-};
-static int g_variant = F32_HERMITE_HORNER | F32_HERMITE_V2 | F32_YUV_NUM | F32_MAP_FMA | F32_PQ_FMA | F32_HLG_FMA;
-
-ORACLE_API void oracle_f32_set_variant(int v) { g_variant = v; }
-ORACLE_API int oracle_f32_get_variant(void) { return g_variant; }
-
-static inline int V(int bit) { return (g_variant & bit) != 0; }
-
-static inline float f_add_mul(float a, float b, float c, int fused) {  /* c + a*b */
-    return fused ? fmaf(a, b, c) : c + a * b;
-}
+/* Where the reference's source leaves it to the compiler, nvcc fuses a product into the
+ * following addition or subtraction (its default -fmad=true).  Which product of a sum of two
+ * products it fuses is not visible in the source; the forms below are the ones that reproduce
+ * the reference's outputs bit for bit on every golden case: the Hermite spline's Horner steps
+ * and its 3*p1 product (resize.hpp:9-22), the Y'CbCr numerators and the G row but not the
+ * constant denominators (YUVToLinRGB.hpp:7-18, 66-94), c2 - c3*a of PQ (transferToLinear.hpp:
+ * 181), HLG's Ys (:49), and s12 - m1*m2 and the SSIM denominator (score.hpp:262-268). */
 
 static inline int64_t imin(int64_t a, int64_t b) { return a < b ? a : b; }
 static inline int64_t imax(int64_t a, int64_t b) { return a > b ? a : b; }
@@ -141,23 +125,16 @@ static Herm herm_make(float p0, float m0, float p1, float m1) {
     Herm h;
     /* v1 = 2*p0 + m0 - 2*p1 + m1: the doublings are exact, so contraction cannot change it */
     h.v1 = ((2.f * p0 + m0) - 2.f * p1) + m1;
-    /* v2 = -3*p0 + 3*p1 - 2*m0 - m1 */
-    float t = V(F32_HERMITE_V2) ? fmaf(p0, -3.f, 3.f * p1)
-            : V(F32_HERMITE_V2_ALT) ? fmaf(p1, 3.f, -3.f * p0) : (-3.f * p0) + (3.f * p1);
+    /* v2 = -3*p0 + 3*p1 - 2*m0 - m1: nvcc rounds -3*p0 and fuses 3*p1 into the sum */
+    const float t = fmaf(p1, 3.f, -3.f * p0);
     h.v2 = (t - 2.f * m0) - m1;
     h.v3 = m0;
     h.v4 = p0;
     return h;
 }
 
-static float herm_get(Herm h, float t) {
-    if (V(F32_HERMITE_HORNER)) return fmaf(fmaf(fmaf(h.v1, t, h.v2), t, h.v3), t, h.v4);
-    float r = h.v1;
-    r *= t; r += h.v2;
-    r *= t; r += h.v3;
-    r *= t; r += h.v4;
-    return r;
-}
+/* get (resize.hpp:14-23): res = v1; res *= t; res += v2; ... as three fused steps. */
+static float herm_get(Herm h, float t) { return fmaf(fmaf(fmaf(h.v1, t, h.v2), t, h.v3), t, h.v4); }
 
 /* getHorizontalInterpolator_device / getVerticalInterpolator_device (:28-50): the four
  * samples around index i of a sequence of n, read through `at(k)`, edge-replicated. */
@@ -240,15 +217,15 @@ static void f_upsample_plane(const float* dec, int64_t sw, int64_t sh, int64_t W
 /* ------------------------------------------------------------------------------------ */
 
 /* The constant denominators vscale*Kr + 0.5f are folded at compile time. */
-static float fold_den(float s, float k) { return V(F32_YUV_DEN) ? fmaf(s, k, 0.5f) : s * k + 0.5f; }
+static float fold_den(float s, float k) { return s * k + 0.5f; }
 
 /* ncl_yuv_to_rgb_from_kr_kb (:7-18); v = (Y, Cb, Cr). */
 static void f_ncl(float v[3], float Kr, float Kb) {
     const float Kg = (1.f - Kb) - Kr;
     const float us = 0.5f / (1.f - Kb), vs = 0.5f / (1.f - Kr);
-    const float r = f_add_mul(v[0], vs, v[2], V(F32_YUV_NUM)) / fold_den(vs, Kr);
-    const float b = f_add_mul(v[0], us, v[1], V(F32_YUV_NUM)) / fold_den(us, Kb);
-    const float g = V(F32_YUV_NUM) ? fmaf(-Kb, b, fmaf(-Kr, r, v[0])) / Kg : ((v[0] - Kr * r) - Kb * b) / Kg;
+    const float r = fmaf(v[0], vs, v[2]) / fold_den(vs, Kr);
+    const float b = fmaf(v[0], us, v[1]) / fold_den(us, Kb);
+    const float g = fmaf(-Kb, b, fmaf(-Kr, r, v[0])) / Kg;
     v[0] = r; v[1] = g; v[2] = b;
 }
 
@@ -261,8 +238,8 @@ static void f_gamma_light(float v[3], Vship_YUVMatrix_t m) {
     case Vship_MATRIX_BT2020_CL: {            /* :77-94 */
         const float Kr = 0.2627f, Kb = 0.0593f;
         const float us = 0.5f / (1.f - Kb), vs = 0.5f / (1.f - Kr);
-        const float r = f_add_mul(v[0], vs, v[2], V(F32_YUV_NUM)) / fold_den(vs, Kr);
-        const float b = f_add_mul(v[0], us, v[1], V(F32_YUV_NUM)) / fold_den(us, Kb);
+        const float r = fmaf(v[0], vs, v[2]) / fold_den(vs, Kr);
+        const float b = fmaf(v[0], us, v[1]) / fold_den(us, Kb);
         v[1] = v[0]; v[0] = r; v[2] = b;
         break;
     }
@@ -279,7 +256,7 @@ static void f_gamma_light(float v[3], Vship_YUVMatrix_t m) {
 static void f_linear_light(float v[3], Vship_YUVMatrix_t m) {
     if (m == Vship_MATRIX_BT2020_CL) {        /* :66-75 */
         const float Kr = 0.2627f, Kb = 0.0593f, Kg = (1.f - Kr) - Kb;
-        v[1] = V(F32_YUV_NUM) ? fmaf(-Kb, v[2], fmaf(-Kr, v[0], v[1])) / Kg : ((v[1] - Kr * v[0]) - Kb * v[2]) / Kg;
+        v[1] = fmaf(-Kb, v[2], fmaf(-Kr, v[0], v[1])) / Kg;
     } else if (m == Vship_MATRIX_BT2100_ICTCP) { /* :28-43 */
         v[0] = fmaf(v[0], 3.4366066943330784267f, fmaf(v[1], -2.5064521186562698975f, v[2] * 0.069845424323191470954f));
         v[1] = fmaf(v[0], -0.23026480071281397f, fmaf(v[1], 1.4064527541936944f, -v[2] * 0.2083538389058436f));
@@ -339,7 +316,7 @@ static void f_trc_array(float* v, int64_t n, Vship_TransferFunction_t t) {
         for (int64_t i = 0; i < n; i++) {
             const float a = res[i];
             const float num = (a - c1) > 0.f ? (a - c1) : 0.f;
-            const float den = V(F32_PQ_FMA) ? fmaf(-c3, a, c2) : c2 - c3 * a;
+            const float den = fmaf(-c3, a, c2);
             arg[i] = num / den;
         }
         g_math(M_POW, arg, 1.f / pn, res, n);
@@ -364,8 +341,8 @@ static void f_hlg_array(float* p, int64_t n) {
     for (int64_t i = 0; i < 3 * n; i++) p[i] = p[i] <= 0.5f ? p[i] * p[i] / 3.f : (res[i] + b) / 12.f;
     for (int64_t i = 0; i < n; i++) {
         const float x = p[i], y = p[n + i], z = p[2 * n + i];
-        const float part = V(F32_HLG_FMA) ? fmaf(0.2627f, x, 0.6780f * y) : 0.2627f * x + 0.6780f * y;
-        const double ys = V(F32_HLG_FMA) ? fma(0.0593, (double)z, (double)part) : (double)part + 0.0593 * (double)z;
+        const float part = fmaf(0.2627f, x, 0.6780f * y);
+        const double ys = fma(0.0593, (double)z, (double)part);
         arg[i] = (float)ys;
     }
     g_math(M_POW, arg, gamma - 1.f, res, n);
@@ -642,14 +619,8 @@ static void f_planescale(const float* a, const float* b, int64_t w, int64_t h,
                     const float s1122 = ssq[i] - 2.f * S12;
                     const float md = M1 - M2;
                     const float num_m = fmaf(md, md * -1.0f, 1.0f);
-                    float num_s, den_s;
-                    if (V(F32_MAP_FMA)) {
-                        num_s = fmaf(fmaf(-M1, M2, S12), 2.0f, 0.0009f);
-                        den_s = fmaf(-M2, M2, fmaf(-M1, M1, s1122)) + 0.0009f;
-                    } else {
-                        num_s = fmaf(S12 - M1 * M2, 2.0f, 0.0009f);
-                        den_s = ((s1122 - M1 * M1) - M2 * M2) + 0.0009f;
-                    }
+                    const float num_s = fmaf(fmaf(-M1, M2, S12), 2.0f, 0.0009f);
+                    const float den_s = fmaf(-M2, M2, fmaf(-M1, M1, s1122)) + 0.0009f;
                     const float q = 1.0f - (num_m * num_s) / den_s;
                     ssim = q > 0.f ? q : 0.f;
                 }

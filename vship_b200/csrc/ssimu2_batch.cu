@@ -353,15 +353,15 @@ __global__ void __launch_bounds__(kMapThreads, TH == 64 ? 3 : 4) ssimu2_batch_ma
     int pair = (int)e0.w;
     unsigned partial = e0.z;
     gate.wait(v, pair);
-    typename MT::Regs regs;
-    load_halo<TH, true, false>(cur, regs);
+    HaloV4T<TH> regs;
+    load_halo_v4t<TH, true>(cur, regs);
     bool have = true;
     for (;;) {
         if (!have) {
             gate.wait(v, pair);
-            load_halo<TH, true, false>(cur, regs);
+            load_halo_v4t<TH, true>(cur, regs);
         }
-        stage_halo<TH, false>(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
+        stage_halo_v4t<TH>(sm, regs, cur.X0, cur.Y0, cur.w, cur.h);
         const TileRef t = cur;
         const unsigned tpartial = partial;
         const int next = m + stride;
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kMapThreads, TH == 64 ? 3 : 4) ssimu2_batch_ma
             // Prefetch only when the next pair's pyramids are complete; otherwise wait after
             // this tile (never while holding it).
             if (gate.ready(v, pair)) {
-                load_halo<TH, true, false>(cur, regs);
+                load_halo_v4t<TH, true>(cur, regs);
                 have = true;
             }
         }

@@ -39,13 +39,16 @@ static __constant__ float c_gauss[17];
 static __constant__ float c_gauss_prefix[18];
 static __constant__ double c_weights[108] = {VSHIP_SSIMU2_WEIGHT_LIST};
 
-// Cube root of max(x, 0): exp2(log2(x) / 3) on the special-function unit refined by one
-// Newton step y <- (2y + x / y^2) / 3, which leaves ~1 ulp of error.
+// Cube root of max(x, 0) without a division: the inverse cube root r = exp2(-log2(x) / 3)
+// on the special-function unit, one Newton step for it, r <- r (4 - x r^3) / 3, then
+// x r^2.  Two special-function operations instead of three (the reciprocal of a Newton step
+// on the cube root itself); ~2 ulp of error.
 __device__ __forceinline__ float fast_cbrt(float x) {
     if (!(x > 0.f)) return 0.f;
-    float y = ex2_approx(__log2f(x) * (1.0f / 3.0f));
-    y = (2.0f * y + __fdividef(x, y * y)) * (1.0f / 3.0f);
-    return y;
+    float r = ex2_approx(__log2f(x) * (-1.0f / 3.0f));
+    const float r3x = x * r * r * r;
+    r = r * (4.0f - r3x) * (1.0f / 3.0f);
+    return x * r * r;
 }
 
 // positive XYB of a linear RGB triple (src/ssimu2/makeXYB.hpp:6-47).
@@ -399,6 +402,74 @@ __device__ __forceinline__ void stage_halo_v4(typename MapTile<kTile>::Smem& sm,
         const int j = tid + it * kMapThreads;
         if (j >= HaloV4::kPos) break;
         const int row = j / HaloV4::kVec, c4 = j - row * HaloV4::kVec;
+        const int gx = X0 - kHalo + 4 * c4;
+        const bool in = (r.inmask >> it) & 1u;
+        const float av[4] = {r.a[it].x, r.a[it].y, r.a[it].z, r.a[it].w};
+        const float bv[4] = {r.b[it].x, r.b[it].y, r.b[it].z, r.b[it].w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const bool ine = in && gx + e < w;
+            sm.sab[row][4 * c4 + e] = ine ? f2(av[e] - k, bv[e] - k) : f2(0.f, 0.f);
+        }
+    }
+    __syncthreads();
+}
+
+// The same 128-bit halo loads for the batch maps kernel, for tile heights 16, 32 and 64 and
+// with coherent (L2) loads (the pyramids were written earlier in the same graph).  The shift
+// constant is exchanged through shared memory: halo element (8, 8), the tile's first output
+// pixel, is position 8 * 12 + 2, component x, held by thread 98.  Registers stay within the
+// kernel's limit: 8, 10 or 16 float4 per thread.
+template <int TH>
+struct HaloV4T {
+    static constexpr int kRows = TH + 2 * kHalo;
+    static constexpr int kVec = kIn / 4;
+    static constexpr int kPos = kRows * kVec;
+    static constexpr int kSlots = (kPos + kMapThreads - 1) / kMapThreads;
+    float4 a[kSlots], b[kSlots];
+    unsigned inmask;
+};
+
+template <int TH, bool kCoherent>
+__device__ __forceinline__ void load_halo_v4t(const TileRef& t, HaloV4T<TH>& r) {
+    using H = HaloV4T<TH>;
+    r.inmask = 0;
+#pragma unroll
+    for (int it = 0; it < H::kSlots; it++) {
+        const int j = threadIdx.x + it * kMapThreads;
+        const int row = j / H::kVec, c4 = j - row * H::kVec;
+        const int gx = t.X0 - kHalo + 4 * c4, gy = t.Y0 - kHalo + row;
+        const bool in = j < H::kPos && gx >= 0 && gx < t.w && gy >= 0 && gy < t.h;
+        const int64_t o = in ? (int64_t)gy * t.pitch + gx : 0;
+        if (kCoherent) {
+            r.a[it] = in ? __ldcg(reinterpret_cast<const float4*>(t.a + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            r.b[it] = in ? __ldcg(reinterpret_cast<const float4*>(t.b + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+            r.a[it] = in ? __ldg(reinterpret_cast<const float4*>(t.a + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            r.b[it] = in ? __ldg(reinterpret_cast<const float4*>(t.b + o)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        r.inmask |= (in ? 1u : 0u) << it;
+    }
+}
+
+template <int TH>
+__device__ __forceinline__ void stage_halo_v4t(typename MapTile<TH>::Smem& sm, const HaloV4T<TH>& r, int X0, int Y0, int w,
+                                               int h) {
+    using H = HaloV4T<TH>;
+    const int tid = threadIdx.x;
+    if (tid < kTile)
+        sm.invx[tid] = 1.0f / blur_norm(min(X0 + tid, w - 1), w);
+    else if (tid < kTile + TH)
+        sm.invy[tid - kTile] = 1.0f / blur_norm(min(Y0 + tid - kTile, h - 1), h);
+    // shift constant: halo element (8, 8) is position 8 * 12 + 2, component 0, held by thread 98
+    if (tid == kHalo * H::kVec + 2) sm.shift = 0.5f * (r.a[0].x + r.b[0].x);
+    __syncthreads();
+    const float k = sm.shift;
+#pragma unroll
+    for (int it = 0; it < H::kSlots; it++) {
+        const int j = tid + it * kMapThreads;
+        if (j >= H::kPos) break;
+        const int row = j / H::kVec, c4 = j - row * H::kVec;
         const int gx = X0 - kHalo + 4 * c4;
         const bool in = (r.inmask >> it) & 1u;
         const float av[4] = {r.a[it].x, r.a[it].y, r.a[it].z, r.a[it].w};
