@@ -142,16 +142,20 @@ __global__ void __launch_bounds__(kMapThreads) ssimu2_maps_kernel(const __grid_c
 __global__ void __launch_bounds__(256) ssimu2_final_kernel(const MapSeg* __restrict__ segs, int segs_per_pair,
                                                            const double* __restrict__ partials,
                                                            double* __restrict__ scores, float* __restrict__ features) {
-    __shared__ double red[8][6];
+    // Every warp walks all segments and leaves its per-segment sums in shared memory, so the
+    // segments need no barrier each; one barrier, then one thread per (segment, map) forms the
+    // feature.  Per thread, per warp and across warps the additions are in the same order as
+    // a segment-by-segment loop, so the sums are the same to the last bit.
+    __shared__ double red[18][8][6];
     __shared__ float feat[108];
     const int pair = blockIdx.x, tid = threadIdx.x;
     for (int i = tid; i < 108; i += 256) feat[i] = 0.f;
-    __syncthreads();
     for (int s = 0; s < segs_per_pair; s++) {
-        const MapSeg sg = segs[pair * segs_per_pair + s];
+        const MapSeg& sg = segs[pair * segs_per_pair + s];
+        const int64_t begin = sg.tile_begin, ntiles = sg.ntiles;
         double acc[6] = {0, 0, 0, 0, 0, 0};
-        for (int t = tid; t < sg.ntiles; t += 256) {
-            const double* p = partials + (int64_t)(sg.tile_begin + t) * 6;
+        for (int t = tid; t < ntiles; t += 256) {
+            const double* p = partials + (begin + t) * 6;
 #pragma unroll
             for (int k = 0; k < 6; k++) acc[k] += p[k];
         }
@@ -162,19 +166,21 @@ __global__ void __launch_bounds__(256) ssimu2_final_kernel(const MapSeg* __restr
         }
         if ((tid & 31) == 0) {
 #pragma unroll
-            for (int k = 0; k < 6; k++) red[tid >> 5][k] = acc[k];
+            for (int k = 0; k < 6; k++) red[s][tid >> 5][k] = acc[k];
         }
-        __syncthreads();
-        if (tid < 3) {
-            const double n = (double)sg.w * (double)sg.h;
-            double s1 = 0.0, s4 = 0.0;
-            for (int w = 0; w < 8; w++) { s1 += red[w][tid]; s4 += red[w][3 + tid]; }
-            const bool on = (sg.on >> tid) & 1;
-            feat[sg.slot + tid] = on ? (float)(s1 / n) : 0.f;
-            feat[sg.slot + 3 + tid] = on ? (float)sqrt(sqrt(s4 / n)) : 0.f;
-        }
-        __syncthreads();
     }
+    __syncthreads();
+    if (tid < 3 * segs_per_pair) {
+        const int s = tid / 3, m = tid - 3 * s;
+        const MapSeg& sg = segs[pair * segs_per_pair + s];
+        const double n = (double)sg.w * (double)sg.h;
+        double s1 = 0.0, s4 = 0.0;
+        for (int w = 0; w < 8; w++) { s1 += red[s][w][m]; s4 += red[s][w][3 + m]; }
+        const bool on = (sg.on >> m) & 1;
+        feat[sg.slot + m] = on ? (float)(s1 / n) : 0.f;
+        feat[sg.slot + 3 + m] = on ? (float)sqrt(sqrt(s4 / n)) : 0.f;
+    }
+    __syncthreads();
     if (features)
         for (int i = tid; i < 108; i += 256) features[(int64_t)pair * 108 + i] = feat[i];
     if (tid == 0) scores[pair] = score_from_features(feat);

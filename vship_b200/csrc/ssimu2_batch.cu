@@ -259,13 +259,14 @@ constexpr int kFinalThreads = 256;
 // Per pair: FP64 totals of the tile partials, the 108 features and the score (the
 // per-handler final kernel's reduction over the pair's segments).
 __global__ void __launch_bounds__(kFinalThreads) ssimu2_batch_final_kernel(const BatchView* __restrict__ vp) {
-    __shared__ double red[kFinalThreads / 32][6];
+    // As the per-handler final kernel: per-segment warp sums in shared memory, one barrier,
+    // one thread per (segment, map); the additions keep the segment-by-segment order.
+    __shared__ double red[18][kFinalThreads / 32][6];
     __shared__ float feat[108];
     const int p = blockIdx.x, tid = threadIdx.x;
     const BatchPair& bp = vp->pairs[p];
     const BatchClass& bc = vp->cls[bp.cls];
     for (int i = tid; i < 108; i += kFinalThreads) feat[i] = 0.f;
-    __syncthreads();
     for (int s = 0; s < bc.nseg; s++) {
         const BatchSeg& g = bc.seg[s];
         double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -281,19 +282,21 @@ __global__ void __launch_bounds__(kFinalThreads) ssimu2_batch_final_kernel(const
         }
         if ((tid & 31) == 0) {
 #pragma unroll
-            for (int k = 0; k < 6; k++) red[tid >> 5][k] = acc[k];
+            for (int k = 0; k < 6; k++) red[s][tid >> 5][k] = acc[k];
         }
-        __syncthreads();
-        if (tid < 3) {
-            const double n = (double)g.w * (double)g.h;
-            double s1 = 0.0, s4 = 0.0;
-            for (int wi = 0; wi < kFinalThreads / 32; wi++) { s1 += red[wi][tid]; s4 += red[wi][3 + tid]; }
-            const bool on = (g.on >> tid) & 1;
-            feat[g.slot + tid] = on ? (float)(s1 / n) : 0.f;
-            feat[g.slot + 3 + tid] = on ? (float)sqrt(sqrt(s4 / n)) : 0.f;
-        }
-        __syncthreads();
     }
+    __syncthreads();
+    if (tid < 3 * bc.nseg) {
+        const int s = tid / 3, m = tid - 3 * s;
+        const BatchSeg& g = bc.seg[s];
+        const double n = (double)g.w * (double)g.h;
+        double s1 = 0.0, s4 = 0.0;
+        for (int wi = 0; wi < kFinalThreads / 32; wi++) { s1 += red[s][wi][m]; s4 += red[s][wi][3 + m]; }
+        const bool on = (g.on >> m) & 1;
+        feat[g.slot + m] = on ? (float)(s1 / n) : 0.f;
+        feat[g.slot + 3 + m] = on ? (float)sqrt(sqrt(s4 / n)) : 0.f;
+    }
+    __syncthreads();
     if (vp->features)
         for (int i = tid; i < 108; i += kFinalThreads) vp->features[(int64_t)p * 108 + i] = feat[i];
     if (tid == 0) vp->scores[p] = score_from_features(feat);
