@@ -172,20 +172,23 @@ __device__ __forceinline__ void blur_tile(BlurSmem<R, NP>& sm, Src src, int X0, 
     else if (tid < 2 * kTile)
         sm.invy[tid - kTile] = 1.0f / tap_sum(K, R, min(Y0 + tid - kTile, h - 1), h);
     __syncthreads();
-    for (int u = tid; u < IN * (kTile / 2); u += 256) {
-        const int r = u >> 4, c0 = (u & 15) * 2;
-        V a0 = B::zero(), a1 = B::zero();
-        V prev = sm.in[r][c0];
+    // Horizontal pass: a work item is four adjacent outputs of one row, each input sample
+    // loaded once and applied to every output whose window holds it (taps in the same order
+    // per output as one output at a time).
+    for (int u = tid; u < IN * (kTile / 4); u += 256) {
+        const int r = u >> 3, c0 = (u & 7) * 4;
+        V a[4] = {B::zero(), B::zero(), B::zero(), B::zero()};
 #pragma unroll
-        for (int j = 0; j < NT; j++) {
-            const float g = c_taps[K][j];
-            const V nxt = sm.in[r][c0 + j + 1];
-            a0 = B::fma(g, prev, a0);
-            a1 = B::fma(g, nxt, a1);
-            prev = nxt;
+        for (int j = 0; j < NT + 3; j++) {
+            const V v = sm.in[r][c0 + j];
+#pragma unroll
+            for (int o = 0; o < 4; o++) {
+                const int t = j - o;
+                if (t >= 0 && t < NT) a[o] = B::fma(c_taps[K][t], v, a[o]);
+            }
         }
-        sm.h[r][c0] = B::scale(a0, sm.invx[c0]);
-        sm.h[r][c0 + 1] = B::scale(a1, sm.invx[c0 + 1]);
+#pragma unroll
+        for (int o = 0; o < 4; o++) sm.h[r][c0 + o] = B::scale(a[o], sm.invx[c0 + o]);
     }
     __syncthreads();
     const int c = tid & 31, r0 = (tid >> 5) * 4;
