@@ -162,10 +162,34 @@ __device__ __forceinline__ void blur_tile(BlurSmem<R, NP>& sm, Src src, int X0, 
     constexpr int IN = BlurSmem<R, NP>::IN;
     constexpr int NT = 2 * R + 1;
     const int tid = threadIdx.x;
-    for (int i = tid; i < IN * IN; i += 256) {
-        const int r = i / IN, c = i % IN;
-        const int gx = X0 - R + c, gy = Y0 - R + r;
-        sm.in[r][c] = (gx >= 0 && gx < w && gy >= 0 && gy < h) ? src(gx, gy) : B::zero();
+    // Staging: warp k takes halo rows k, k + 8, ...; lane l columns l, l + 32, l + 64 of a
+    // row, so each row's bounds test and base address are computed once and a warp's stores
+    // fall in one row (no bank conflicts).  Two rows per step, all loads before the stores.
+    {
+        constexpr int kCols = (IN + 31) / 32;
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int r0 = warp; r0 < IN; r0 += 16) {
+            V v[2][kCols];
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int r = r0 + 8 * s;
+                const int gy = Y0 - R + r;
+                const bool rowin = r < IN && (unsigned)gy < (unsigned)h;
+#pragma unroll
+                for (int k = 0; k < kCols; k++) {
+                    const int c = lane + 32 * k, gx = X0 - R + c;
+                    v[s][k] = (rowin && c < IN && (unsigned)gx < (unsigned)w) ? src(gx, gy) : B::zero();
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int r = r0 + 8 * s;
+                if (r >= IN) break;
+#pragma unroll
+                for (int k = 0; k < kCols; k++)
+                    if (lane + 32 * k < IN) sm.in[r][lane + 32 * k] = v[s][k];
+            }
+        }
     }
     if (tid < kTile)
         sm.invx[tid] = 1.0f / tap_sum(K, R, min(X0 + tid, w - 1), w);
