@@ -51,6 +51,19 @@ __device__ __forceinline__ float fast_cbrt(float x) {
     return x * r * r;
 }
 
+// fast_cbrt(x) + add for two values, with the multiplies and adds in packed FP32x2 (one issue
+// slot per pair).  4 - x r^3 and x r^2 + add are single fused operations, as the compiler
+// contracts them in the scalar form (fast_cbrt inlined into positive_xyb).
+__device__ __forceinline__ float2 fast_cbrt2_add(float2 x, float add) {
+    const float2 e = __fmul2_rn(make_float2(__log2f(x.x), __log2f(x.y)), make_float2(-1.0f / 3.0f, -1.0f / 3.0f));
+    float2 r = make_float2(ex2_approx(e.x), ex2_approx(e.y));
+    const float2 xrr = __fmul2_rn(__fmul2_rn(x, r), r);
+    const float2 t = __ffma2_rn(make_float2(-xrr.x, -xrr.y), r, make_float2(4.0f, 4.0f));
+    r = __fmul2_rn(__fmul2_rn(r, t), make_float2(1.0f / 3.0f, 1.0f / 3.0f));
+    const float2 y = __ffma2_rn(__fmul2_rn(x, r), r, make_float2(add, add));
+    return make_float2(x.x > 0.f ? y.x : add, x.y > 0.f ? y.y : add);
+}
+
 // positive XYB of a linear RGB triple (src/ssimu2/makeXYB.hpp:6-47).
 __device__ __forceinline__ float3 positive_xyb(float3 a) {
     const float bias = 0.0037930734f;
@@ -58,8 +71,9 @@ __device__ __forceinline__ float3 positive_xyb(float3 a) {
     float m = fmaf(0.23f, a.x, fmaf(0.692f, a.y, fmaf(0.078f, a.z, bias)));
     float s = fmaf(0.24342269f, a.x, fmaf(0.20476745f, a.y, fmaf(0.55180986f, a.z, bias)));
     const float absb = -0.1559542025327239f;
-    l = fast_cbrt(l) + absb;
-    m = fast_cbrt(m) + absb;
+    const float2 lm = fast_cbrt2_add(make_float2(l, m), absb);
+    l = lm.x;
+    m = lm.y;
     s = fast_cbrt(s) + absb;
     const float X = 0.5f * (l - m);
     const float Y = X + m;
