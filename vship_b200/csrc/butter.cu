@@ -326,38 +326,152 @@ __global__ void __launch_bounds__(256) opsin_kernel(Planes P) {
     }
 }
 
-// Low-frequency split (separatefrequencies.hpp:160-176, XybLowFreqToVals :3-12).
-// Three scalar passes: a packed two-plane tile of radius 21 needs 64 KB of shared memory and
-// the occupancy it costs outweighs the halved tap arithmetic (measured 1.06 against 0.99 ms
-// per 4K pair).
-__global__ void __launch_bounds__(256) lf_kernel(Planes P) {
-    __shared__ BlurSmem<21, 1> sm;
-    const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kTile;
-    float bl[3][4];
-    const int w = P.w;
+// Low-frequency split (separatefrequencies.hpp:160-176, XybLowFreqToVals :3-12) as two
+// passes of the radius-21 blur through an intermediate plane, as the reference runs it
+// (separate horizontal and vertical kernels for radii above 8, gaussianblur.hpp:60-250): a
+// 32x32 tile of the fused form blurs 74 halo rows horizontally for 32 output rows and stages
+// 74^2 samples for 1,024 outputs, while the row pass blurs each row once and the column pass
+// stages 106 rows for 64.  Measured per 4K pair: 0.64 ms against 0.68 for the tiled form (the
+// pass is latency-bound; five column-pass CTAs per SM, 48 registers, beat fewer CTAs with
+// more rows per thread).  The intermediate lives in the mf planes, which the mf kernel
+// writes only afterwards.  Per output, the taps and the renormalisation are applied in the
+// same order as in blur_tile, so the values are those of the tiled blur.
+constexpr int kLfR = 21;
+constexpr int kLfNT = 2 * kLfR + 1;
+constexpr int kLfK = 4;                 // tap set of sigma 7.16
+constexpr int kLfHW = 128;              // row pass: 32 rows x 128 columns per CTA
+constexpr int kLfHIn = kLfHW + 2 * kLfR;
+constexpr int kLfVRows = 64;            // column pass: 64 rows x 32 columns per CTA
+constexpr int kLfRPT = kLfVRows / 8;    // rows per thread
+constexpr int kLfVIn = kLfVRows + 2 * kLfR;
+
+struct LfRowSmem {
+    float in[32][kLfHIn + 1];   // odd pitch: lanes on consecutive rows read without conflicts
+    float out[32][kLfHW + 1];
+    float invx[kLfHW];
+};
+
+// Row pass of plane blockIdx.z: xyb -> mf (horizontal blur, renormalised per column).
+__global__ void __launch_bounds__(256) lf_row_kernel(Planes P) {
+    __shared__ LfRowSmem sm;
+    const int c = blockIdx.z;
+    const int X0 = blockIdx.x * kLfHW, Y0 = blockIdx.y * 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int w = P.w, h = P.h;
+    const float* src = P.xyb[c];
+    // Staging: warp k takes rows k, k + 8, k + 16, k + 24; lanes the columns.
+    constexpr int kCols = (kLfHIn + 31) / 32;
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const float* src = P.xyb[c];
-        blur_tile<21, 4, 1>(sm, [&](int x, int y) { return src[(int64_t)y * w + x]; }, X0, Y0, P.w, P.h, bl[c]);
+    for (int s = 0; s < 4; s++) {
+        const int r = warp + 8 * s, gy = Y0 + r;
+        const bool rowin = gy < h;
+        const float* row = src + (int64_t)(rowin ? gy : 0) * w;
+        float v[kCols];
+#pragma unroll
+        for (int k = 0; k < kCols; k++) {
+            const int cc = lane + 32 * k, gx = X0 - kLfR + cc;
+            v[k] = (rowin && cc < kLfHIn && (unsigned)gx < (unsigned)w) ? row[gx] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < kCols; k++)
+            if (lane + 32 * k < kLfHIn) sm.in[r][lane + 32 * k] = v[k];
     }
-    const int c = threadIdx.x & 31, r0 = (threadIdx.x >> 5) * 4;
-    const int x = X0 + c;
-    if (x >= P.w) return;
+    if (tid < kLfHW) sm.invx[tid] = 1.0f / tap_sum(kLfK, kLfR, min(X0 + tid, w - 1), w);
+    __syncthreads();
+    // A work item is four adjacent outputs of one row; consecutive threads take consecutive rows.
+    for (int u = tid; u < 32 * (kLfHW / 4); u += 256) {
+        const int r = u & 31, c0 = (u >> 5) * 4;
+        float a[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-    for (int o = 0; o < 4; o++) {
-        const int y = Y0 + r0 + o;
-        if (y >= P.h) break;
-        const int64_t i = (int64_t)y * P.w + x;
-        float vx = bl[0][o], vy = bl[1][o], vb = bl[2][o];
+        for (int j = 0; j < kLfNT + 3; j++) {
+            const float v = sm.in[r][c0 + j];
 #pragma unroll
-        for (int k = 0; k < 3; k++) P.d[k][i] = P.xyb[k][i] - bl[k][o];
-        vb = vb + -0.362267051518f * vy;
-        vb = vb * 49.87984651440f;
-        vx = vx * 33.832837186260f;
-        vy = vy * 14.458268100570f;
-        P.lf[0][i] = vx;
-        P.lf[1][i] = vy;
-        P.lf[2][i] = vb;
+            for (int o = 0; o < 4; o++) {
+                const int t = j - o;
+                if (t >= 0 && t < kLfNT) a[o] = fmaf(v, c_taps[kLfK][t], a[o]);
+            }
+        }
+#pragma unroll
+        for (int o = 0; o < 4; o++) sm.out[r][c0 + o] = a[o] * sm.invx[c0 + o];
+    }
+    __syncthreads();
+    float* dst = P.mf[c];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        const int r = warp + 8 * s, gy = Y0 + r;
+        if (gy >= h) break;
+#pragma unroll
+        for (int k = 0; k < kLfHW / 32; k++) {
+            const int gx = X0 + lane + 32 * k;
+            if (gx < w) dst[(int64_t)gy * w + gx] = sm.out[r][lane + 32 * k];
+        }
+    }
+}
+
+// Column pass: mf (row-blurred) -> the low-frequency values lf and xyb - blur, for the three
+// planes in turn (plane 2's value needs plane 1's blur).  Thread t: column t & 31, rows
+// kLfRPT (t >> 5) .. + kLfRPT - 1 of the CTA's kLfVRows.
+__global__ void __launch_bounds__(256, 5) lf_col_kernel(Planes P) {
+    __shared__ float hs[kLfVIn][kTile + 1];
+    __shared__ float invy[kLfVRows];
+    const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kLfVRows;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int w = P.w, h = P.h;
+    const int x = X0 + lane, r0 = warp * kLfRPT;
+    if (tid < kLfVRows) invy[tid] = 1.0f / tap_sum(kLfK, kLfR, min(Y0 + tid, h - 1), h);
+    float by[kLfRPT];
+#pragma unroll 1
+    for (int c = 0; c < 3; c++) {
+        if (c) __syncthreads();  // the previous plane's pass has read hs
+        const float* src = P.mf[c];
+        for (int rb = warp; rb < kLfVIn; rb += 32) {
+            float v[4];
+#pragma unroll
+            for (int s = 0; s < 4; s++) {
+                const int r = rb + 8 * s, gy = Y0 - kLfR + r;
+                v[s] = (r < kLfVIn && (unsigned)gy < (unsigned)h && x < w) ? src[(int64_t)gy * w + x] : 0.f;
+            }
+#pragma unroll
+            for (int s = 0; s < 4; s++)
+                if (rb + 8 * s < kLfVIn) hs[rb + 8 * s][lane] = v[s];
+        }
+        __syncthreads();
+        float acc[kLfRPT];
+#pragma unroll
+        for (int o = 0; o < kLfRPT; o++) acc[o] = 0.f;
+#pragma unroll
+        for (int j = 0; j < kLfNT + kLfRPT - 1; j++) {
+            const float v = hs[r0 + j][lane];
+#pragma unroll
+            for (int o = 0; o < kLfRPT; o++) {
+                const int t = j - o;
+                if (t >= 0 && t < kLfNT) acc[o] = fmaf(v, c_taps[kLfK][t], acc[o]);
+            }
+        }
+        if (x >= w) continue;
+#pragma unroll
+        for (int o = 0; o < kLfRPT; o++) {
+            const int y = Y0 + r0 + o;
+            if (y >= h) break;
+            const int64_t i = (int64_t)y * w + x;
+            const float bl = acc[o] * invy[r0 + o];
+            P.d[c][i] = P.xyb[c][i] - bl;
+            if (c == 0) {
+                float vx = bl;
+                vx = vx * 33.832837186260f;
+                P.lf[0][i] = vx;
+            } else if (c == 1) {
+                by[o] = bl;
+                float vy = bl;
+                vy = vy * 14.458268100570f;
+                P.lf[1][i] = vy;
+            } else {
+                float vb = bl;
+                vb = vb + -0.362267051518f * by[o];
+                vb = vb * 49.87984651440f;
+                P.lf[2][i] = vb;
+            }
+        }
     }
 }
 
@@ -856,7 +970,9 @@ private:
             CUDA_CHECK(cudaGetLastError());
             timer_.end(t, st);
             t = timer_.begin(1, "butter_lf", st);
-            lf_kernel<<<grid, 256, 0, st>>>(P[im]);
+            lf_row_kernel<<<dim3((unsigned)ceil_div(w, kLfHW), (unsigned)ceil_div(h, 32), 3u), 256, 0, st>>>(P[im]);
+            CUDA_CHECK(cudaGetLastError());
+            lf_col_kernel<<<dim3((unsigned)ceil_div(w, kTile), (unsigned)ceil_div(h, kLfVRows)), 256, 0, st>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
             timer_.end(t, st);
             t = timer_.begin(2, "butter_mf", st);
