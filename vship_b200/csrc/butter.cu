@@ -3,10 +3,11 @@
 // The reference (src/butter/main.hpp:25-231) runs about 60 kernels per scale and image
 // pair, each a full-plane pass: separable blurs as separate horizontal and vertical kernels
 // and every band/diff/mask step as its own pointwise kernel.  This engine fuses the path into
-// seven kernels per scale:
+// eight kernels per scale:
 //
 //   per image:  opsin    blur(sigma 1.2) of linear RGB + opsin dynamics          -> XYB
-//               lf       blur(sigma 7.16, radius 21) of XYB + low-frequency vals  -> lf, XYB-lf
+//               lf       blur(sigma 7.16, radius 21) of XYB in a row and a column pass,
+//                        + low-frequency vals                                     -> lf, XYB-lf
 //               mf       blur(sigma 3.22, radius 9) + mf range shaping + X-by-Y suppression
 //               hf       blur(sigma 1.56) + hf/uhf split + psycho-mask precompute
 //               mask     blur(sigma 2.7) of the mask precompute
@@ -15,9 +16,9 @@
 //   final:      norms    2x supersampled combination of both scales, optional distmap
 //                        output, FP64 partial sums of d^Q, |d|^3 and max|d|
 //
-// Every blur is a tiled separable renormalised truncated Gaussian: a (32+2R)^2 input tile in
-// shared memory (zero outside the image), the horizontal pass into a second shared tile,
-// the vertical pass into registers, each pass divided by the sum of its in-bounds taps
+// Every blur but lf's is a tiled separable renormalised truncated Gaussian: a (32+2R)^2 input
+// tile in shared memory (zero outside the image), the horizontal pass into a second shared
+// tile, the vertical pass into registers, each pass divided by the sum of its in-bounds taps
 // (src/butter/gaussianblur.hpp:59-187).  All storage and arithmetic is FP32, as in the
 // reference; only the norm sums are FP64.
 #include <cuda_runtime.h>
