@@ -863,6 +863,9 @@ public:
         generic_ = geo_[0].generic() || geo_[1].generic();
         CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         CUDA_CHECK(cudaEventCreateWithFlags(&last_done_, cudaEventDisableTiming));
+        CUDA_CHECK(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
+        CUDA_CHECK(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+        CUDA_CHECK(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
         upload_constants();
         for (int c = 0; c < 2; c++) {
             int64_t off[3];
@@ -962,33 +965,44 @@ private:
         if (!distmap_d_) distmap_d_ = device_alloc<float>((size_t)w_ * h_, "distortion map");
     }
 
-    void scale_pass(int w, int h, bool half, float* out, cudaStream_t st) {
+    // Orders `to` after the work enqueued so far on `from`.
+    void after(cudaStream_t to, cudaStream_t from, cudaEvent_t ev) {
+        CUDA_CHECK(cudaEventRecord(ev, from));
+        CUDA_CHECK(cudaStreamWaitEvent(to, ev, 0));
+    }
+
+    // One scale: the per-image kernels of the reference image on `st` and of the distorted
+    // image on `aux`, concurrently (they share no planes), then the diff map on `st` once both
+    // are done.  The caller has ordered `aux` after the inputs of this scale.
+    void scale_pass(int w, int h, bool half, float* out, cudaStream_t st, cudaStream_t aux) {
         const dim3 grid((unsigned)ceil_div(w, kTile), (unsigned)ceil_div(h, kTile));
         Planes P[2] = {planes_of(0, w, h, half), planes_of(1, w, h, half)};
         for (int im = 0; im < 2; im++) {
-            int t = timer_.begin(0, "butter_opsin", st);
-            opsin_kernel<<<grid, 256, 0, st>>>(P[im]);
+            const cudaStream_t si = im ? aux : st;
+            int t = timer_.begin(0, "butter_opsin", si);
+            opsin_kernel<<<grid, 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
-            timer_.end(t, st);
-            t = timer_.begin(1, "butter_lf", st);
-            lf_row_kernel<<<dim3((unsigned)ceil_div(w, kLfHW), (unsigned)ceil_div(h, 32), 3u), 256, 0, st>>>(P[im]);
+            timer_.end(t, si);
+            t = timer_.begin(1, "butter_lf", si);
+            lf_row_kernel<<<dim3((unsigned)ceil_div(w, kLfHW), (unsigned)ceil_div(h, 32), 3u), 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
-            lf_col_kernel<<<dim3((unsigned)ceil_div(w, kTile), (unsigned)ceil_div(h, kLfVRows)), 256, 0, st>>>(P[im]);
+            lf_col_kernel<<<dim3((unsigned)ceil_div(w, kTile), (unsigned)ceil_div(h, kLfVRows)), 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
-            timer_.end(t, st);
-            t = timer_.begin(2, "butter_mf", st);
-            mf_kernel<<<grid, 256, 0, st>>>(P[im]);
+            timer_.end(t, si);
+            t = timer_.begin(2, "butter_mf", si);
+            mf_kernel<<<grid, 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
-            timer_.end(t, st);
-            t = timer_.begin(3, "butter_hf", st);
-            hf_kernel<<<grid, 256, 0, st>>>(P[im]);
+            timer_.end(t, si);
+            t = timer_.begin(3, "butter_hf", si);
+            hf_kernel<<<grid, 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
-            timer_.end(t, st);
-            t = timer_.begin(4, "butter_mask", st);
-            mask_kernel<<<grid, 256, 0, st>>>(P[im]);
+            timer_.end(t, si);
+            t = timer_.begin(4, "butter_mask", si);
+            mask_kernel<<<grid, 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
-            timer_.end(t, st);
+            timer_.end(t, si);
         }
+        after(st, aux, join_);
         DiffArgs d{};
         d.w = w;
         d.h = h;
@@ -1010,14 +1024,20 @@ private:
 
     void run(const RawImage raw[2], const ColourParams cp[2], cudaStream_t st, double* norms_d, float* distmap, int64_t dst_pitch) {
         const int64_t n0 = (int64_t)w_ * h_;
+        // The two images' colour conversion, downsampling and per-image kernels run on two
+        // streams (image 0 on st, image 1 on the second stream) and meet before each diff
+        // map.  With per-kernel timing on, both run on st, so each timed stage runs alone.
+        const cudaStream_t aux = timer_.enabled ? st : aux_;
+        after(aux, st, fork_);
         for (int c = 0; c < 2; c++) {
+            const cudaStream_t si = c ? aux : st;
             float* lin = plane(c, 0);
             if (!generic_) {
-                launch_ingest_linear(raw[c], cp[c], lin, plane_floats_, st);
+                launch_ingest_linear(raw[c], cp[c], lin, plane_floats_, si);
             } else {
-                lin_generic_[c].run(raw[c], cp[c], geo_[c], st);
+                lin_generic_[c].run(raw[c], cp[c], geo_[c], si);
                 const float* win = lin_generic_[c].planes + (int64_t)geo_[c].crop_top * geo_[c].TW + geo_[c].crop_left;
-                copy_window_kernel<<<(unsigned)ceil_div(n0, 256), 256, 0, st>>>(win, geo_[c].TW, geo_[c].TW * geo_[c].TH,
+                copy_window_kernel<<<(unsigned)ceil_div(n0, 256), 256, 0, si>>>(win, geo_[c].TW, geo_[c].TW * geo_[c].TH,
                                                                                  lin, plane_floats_, w_, h_);
                 CUDA_CHECK(cudaGetLastError());
             }
@@ -1026,11 +1046,13 @@ private:
         for (int c = 0; c < 2; c++)
             for (int k = 0; k < 3; k++) {
                 const dim3 g((unsigned)ceil_div(w1, 16), (unsigned)ceil_div(h1, 16));
-                downsample_kernel<<<g, dim3(16, 16), 0, st>>>(plane(c, k), plane(c, 3 + k), w_, h_);
+                downsample_kernel<<<g, dim3(16, 16), 0, c ? aux : st>>>(plane(c, k), plane(c, 3 + k), w_, h_);
                 CUDA_CHECK(cudaGetLastError());
             }
-        scale_pass(w_, h_, false, diffmap(0), st);
-        scale_pass(w1, h1, true, diffmap(1), st);
+        scale_pass(w_, h_, false, diffmap(0), st, aux);
+        // The half scale reuses the full scale's band planes, which the full-scale diff map reads.
+        after(aux, st, fork_);
+        scale_pass(w1, h1, true, diffmap(1), st, aux);
         const int t = timer_.begin(6, "butter_norms", st);
         combine_norms_kernel<<<nblocks_, 256, 0, st>>>(diffmap(0), diffmap(1), w_, h_, w1, qnorm_, distmap, dst_pitch, partials_);
         CUDA_CHECK(cudaGetLastError());
@@ -1056,6 +1078,14 @@ private:
             (void)cudaEventDestroy(last_done_);
             last_done_ = nullptr;
         }
+        if (fork_) (void)cudaEventDestroy(fork_);
+        if (join_) (void)cudaEventDestroy(join_);
+        fork_ = join_ = nullptr;
+        if (aux_) {
+            (void)cudaStreamSynchronize(aux_);
+            (void)cudaStreamDestroy(aux_);
+            aux_ = nullptr;
+        }
         if (stream_) {
             (void)cudaStreamDestroy(stream_);
             stream_ = nullptr;
@@ -1080,6 +1110,8 @@ private:
     double* norms_host_ = nullptr;
     float* distmap_d_ = nullptr;
     cudaEvent_t last_done_ = nullptr;  // completion of the previous call, on whichever stream it ran
+    cudaStream_t aux_ = nullptr;       // second stream: the distorted image's per-image kernels
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
     KernelTimer timer_;
 };
 
