@@ -58,3 +58,37 @@ def test_device_api_matches_host_api(gpu):
         torch.cuda.synchronize()
         np.testing.assert_array_equal(norms.cpu().numpy(), np.array(host))
         np.testing.assert_array_equal(dmap[:, :w].cpu().numpy(), hmap)
+
+
+def test_concurrent_handlers_on_own_streams(gpu):
+    """Several handlers, each on its own stream, calls interleaved from one thread (the bench's
+    device-throughput method), and the legacy default stream: norms and distortion maps equal
+    the host API's bit for bit.  Each handler also forks its distorted image onto a second
+    stream internally, so this covers both levels of concurrency."""
+    import torch
+    w, h = 517, 301
+    pairs = synth.make_pairs(4, w, h, fmt="rgb8", seed=12, blur=(0.0, 1.5))
+    cs = abi.srgb8(w, h)
+    ls = pairs[0][2]
+    with api.Butteraugli(cs, qnorm=5, intensity=203.0) as hh:
+        expect = [hh.compute(p1, p2, ls, distmap=True) for p1, p2, _ in pairs]
+    dev = [([torch.from_numpy(p.copy()).cuda() for p in p1], [torch.from_numpy(p.copy()).cuda() for p in p2])
+           for p1, p2, _ in pairs]
+    hs = [api.Butteraugli(cs, qnorm=5, intensity=203.0) for _ in range(3)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream(), None]  # None: the legacy default stream
+    try:
+        norms = torch.zeros(len(pairs), 3, dtype=torch.float64, device="cuda")
+        maps = torch.zeros(len(pairs), h, w, dtype=torch.float32, device="cuda")
+        for rep in range(2):
+            for i, (d1, d2) in enumerate(dev):
+                k = (i + rep) % 3
+                s = streams[k]
+                hs[k].compute_device([t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls, ls,
+                                     norms[i].data_ptr(), maps[i].data_ptr(), w * 4, s.cuda_stream if s else 0)
+            torch.cuda.synchronize()
+            for i, (en, em) in enumerate(expect):
+                np.testing.assert_array_equal(norms[i].cpu().numpy(), np.array(en))
+                np.testing.assert_array_equal(maps[i].cpu().numpy(), em)
+    finally:
+        for x in hs:
+            x.close()

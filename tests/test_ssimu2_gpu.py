@@ -173,3 +173,31 @@ def test_device_path_with_odd_plane_addresses(gpu):
         hb.compute_device(a, b, ls, ls, norms.data_ptr())
         torch.cuda.synchronize()
     assert tuple(norms.cpu().numpy()) == tuple(bwant), (norms.cpu().numpy(), bwant)
+
+
+def test_concurrent_handlers_on_own_streams(gpu):
+    """Single-pair device calls dealt round-robin over handlers, each on its own stream (the
+    bench's device-throughput method for one pair per call): every score equals the host API's."""
+    import torch
+    w, h = 640, 360
+    pairs = synth.make_pairs(6, w, h, fmt="rgb8", seed=21)
+    cs = abi.srgb8(w, h)
+    ls = pairs[0][2]
+    with api.SSIMU2(cs) as hh:
+        expect = [hh.compute(p1, p2, ls, ls) for p1, p2, _ in pairs]
+    dev = [([torch.from_numpy(p.copy()).cuda() for p in p1], [torch.from_numpy(p.copy()).cuda() for p in p2])
+           for p1, p2, _ in pairs]
+    hs = [api.SSIMU2(cs) for _ in range(4)]
+    streams = [torch.cuda.Stream() for _ in range(4)]
+    try:
+        out = torch.zeros(len(pairs), dtype=torch.float64, device="cuda")
+        for rep in range(3):
+            for i, (d1, d2) in enumerate(dev):
+                k = (i + rep) % 4
+                hs[k].compute_device(1, [t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls, ls,
+                                     out[i:i + 1].data_ptr(), 0, streams[k].cuda_stream)
+            torch.cuda.synchronize()
+            assert out.cpu().numpy().tolist() == expect
+    finally:
+        for x in hs:
+            x.close()

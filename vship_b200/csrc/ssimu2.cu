@@ -154,6 +154,8 @@ __global__ void __launch_bounds__(256) ssimu2_final_kernel(const MapSeg* __restr
         const MapSeg& sg = segs[pair * segs_per_pair + s];
         const int64_t begin = sg.tile_begin, ntiles = sg.ntiles;
         double acc[6] = {0, 0, 0, 0, 0, 0};
+        // Unrolled so that several tiles' loads are in flight; the additions stay in tile order.
+#pragma unroll 4
         for (int t = tid; t < ntiles; t += 256) {
             const double* p = partials + (begin + t) * 6;
 #pragma unroll

@@ -270,6 +270,7 @@ __global__ void __launch_bounds__(kFinalThreads) ssimu2_batch_final_kernel(const
     for (int s = 0; s < bc.nseg; s++) {
         const BatchSeg& g = bc.seg[s];
         double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 4
         for (int t = tid; t < g.ntiles; t += kFinalThreads) {
             const double* q = vp->partials + (bp.partial + g.tile_begin + t) * 6;
 #pragma unroll
