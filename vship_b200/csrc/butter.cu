@@ -21,6 +21,7 @@
 // tile, the vertical pass into registers, each pass divided by the sum of its in-bounds taps
 // (src/butter/gaussianblur.hpp:59-187).  All storage and arithmetic is FP32, as in the
 // reference; only the norm sums are FP64.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstring>
@@ -409,16 +410,63 @@ __global__ void __launch_bounds__(256) lf_row_kernel(Planes P) {
     }
 }
 
-// Column pass: mf (row-blurred) -> the low-frequency values lf and xyb - blur, for the three
-// planes in turn (plane 2's value needs plane 1's blur).  Thread t: column t & 31, rows
-// kLfRPT (t >> 5) .. + kLfRPT - 1 of the CTA's kLfVRows.
+// Vertical pass of plane c over a staged box (kLfVIn rows of 32 columns, row pitch PITCH
+// floats) and the low-frequency epilogue: lf and xyb - blur.  Thread t: column t & 31, rows
+// kLfRPT (t >> 5) .. + kLfRPT - 1 of the CTA's kLfVRows.  Plane 2's value needs plane 1's blur,
+// which the caller keeps in by[] between the calls.
+template <int PITCH>
+__device__ __forceinline__ void lf_col_plane(const Planes& P, const float* box, const float* invy, int c, int X0,
+                                             int Y0, float (&by)[kLfRPT]) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int w = P.w, h = P.h;
+    const int x = X0 + lane, r0 = warp * kLfRPT;
+    float acc[kLfRPT];
+#pragma unroll
+    for (int o = 0; o < kLfRPT; o++) acc[o] = 0.f;
+#pragma unroll
+    for (int j = 0; j < kLfNT + kLfRPT - 1; j++) {
+        const float v = box[(r0 + j) * PITCH + lane];
+#pragma unroll
+        for (int o = 0; o < kLfRPT; o++) {
+            const int t = j - o;
+            if (t >= 0 && t < kLfNT) acc[o] = fmaf(v, c_taps[kLfK][t], acc[o]);
+        }
+    }
+    if (x >= w) return;
+#pragma unroll
+    for (int o = 0; o < kLfRPT; o++) {
+        const int y = Y0 + r0 + o;
+        if (y >= h) break;
+        const int64_t i = (int64_t)y * w + x;
+        const float bl = acc[o] * invy[r0 + o];
+        P.d[c][i] = P.xyb[c][i] - bl;
+        if (c == 0) {
+            float vx = bl;
+            vx = vx * 33.832837186260f;
+            P.lf[0][i] = vx;
+        } else if (c == 1) {
+            by[o] = bl;
+            float vy = bl;
+            vy = vy * 14.458268100570f;
+            P.lf[1][i] = vy;
+        } else {
+            float vb = bl;
+            vb = vb + -0.362267051518f * by[o];
+            vb = vb * 49.87984651440f;
+            P.lf[2][i] = vb;
+        }
+    }
+}
+
+// Column pass: mf (row-blurred) -> lf and xyb - blur for the three planes in turn, each box
+// staged with plain loads into a padded shared tile (any plane width).
 __global__ void __launch_bounds__(256, 5) lf_col_kernel(Planes P) {
     __shared__ float hs[kLfVIn][kTile + 1];
     __shared__ float invy[kLfVRows];
     const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kLfVRows;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int w = P.w, h = P.h;
-    const int x = X0 + lane, r0 = warp * kLfRPT;
+    const int x = X0 + lane;
     if (tid < kLfVRows) invy[tid] = 1.0f / tap_sum(kLfK, kLfR, min(Y0 + tid, h - 1), h);
     float by[kLfRPT];
 #pragma unroll 1
@@ -437,40 +485,80 @@ __global__ void __launch_bounds__(256, 5) lf_col_kernel(Planes P) {
                 if (rb + 8 * s < kLfVIn) hs[rb + 8 * s][lane] = v[s];
         }
         __syncthreads();
-        float acc[kLfRPT];
-#pragma unroll
-        for (int o = 0; o < kLfRPT; o++) acc[o] = 0.f;
-#pragma unroll
-        for (int j = 0; j < kLfNT + kLfRPT - 1; j++) {
-            const float v = hs[r0 + j][lane];
-#pragma unroll
-            for (int o = 0; o < kLfRPT; o++) {
-                const int t = j - o;
-                if (t >= 0 && t < kLfNT) acc[o] = fmaf(v, c_taps[kLfK][t], acc[o]);
-            }
+        lf_col_plane<kTile + 1>(P, &hs[0][0], invy, c, X0, Y0, by);
+    }
+}
+
+// The same column pass with each plane's box brought into shared memory by the tensor-memory
+// accelerator (a tiled cp.async.bulk.tensor load of this GPU's own mf plane, no multicast),
+// double-buffered across the three planes: plane c + 2's box loads while plane c + 1 is
+// blurred.  The box is dense (32 floats per row), which suits this pass: a warp reads one row
+// of it at a time, so no padding is needed against bank conflicts.  The box origin's x is a
+// multiple of 32 floats (128 bytes); rows above and below the plane read as zero (the tensor
+// map's out-of-bounds fill), as do columns past its width.  Used when the plane's row pitch
+// (its width in bytes) is a multiple of 16, which a tensor map requires.
+struct LfColMaps {
+    CUtensorMap m[3];  // the three mf planes of one image at one scale, box 32 x kLfVIn
+};
+
+constexpr unsigned kLfBoxBytes = kLfVIn * kTile * sizeof(float);
+constexpr long long kTmaWaitLimit = 1ll << 24;  // polls of a box's barrier before giving up
+
+__device__ __forceinline__ void lf_box_load(const CUtensorMap* map, float* dst, uint64_t* bar, int x, int y) {
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kLfBoxBytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(b)
+        : "memory");
+}
+
+// Polls the barrier's phase `parity` at most kTmaWaitLimit times; false if it did not complete.
+__device__ __forceinline__ bool lf_box_wait(uint64_t* bar, unsigned parity) {
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    for (long long i = 0; i < kTmaWaitLimit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done) : "r"(b), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(256, 5) lf_col_tma_kernel(Planes P, const __grid_constant__ LfColMaps maps,
+                                                            int* __restrict__ err) {
+    __shared__ alignas(128) float box[2][kLfVIn * kTile];
+    __shared__ float invy[kLfVRows];
+    __shared__ alignas(8) uint64_t bar[2];
+    __shared__ int ok[3];
+    const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kLfVRows;
+    const int tid = threadIdx.x, h = P.h;
+    if (tid == 0) {
+        for (int b = 0; b < 2; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&bar[b])) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        lf_box_load(&maps.m[0], box[0], &bar[0], X0, Y0 - kLfR);
+        lf_box_load(&maps.m[1], box[1], &bar[1], X0, Y0 - kLfR);
+    }
+    if (tid < kLfVRows) invy[tid] = 1.0f / tap_sum(kLfK, kLfR, min(Y0 + tid, h - 1), h);
+    float by[kLfRPT];
+#pragma unroll 1
+    for (int c = 0; c < 3; c++) {
+        const int b = c & 1;
+        // One thread waits for the box; the barrier then hands its data to the whole CTA.
+        if (tid == 0) {
+            ok[c] = lf_box_wait(&bar[b], (unsigned)(c >> 1));
+            if (!ok[c]) atomicExch(err, 1);
         }
-        if (x >= w) continue;
-#pragma unroll
-        for (int o = 0; o < kLfRPT; o++) {
-            const int y = Y0 + r0 + o;
-            if (y >= h) break;
-            const int64_t i = (int64_t)y * w + x;
-            const float bl = acc[o] * invy[r0 + o];
-            P.d[c][i] = P.xyb[c][i] - bl;
-            if (c == 0) {
-                float vx = bl;
-                vx = vx * 33.832837186260f;
-                P.lf[0][i] = vx;
-            } else if (c == 1) {
-                by[o] = bl;
-                float vy = bl;
-                vy = vy * 14.458268100570f;
-                P.lf[1][i] = vy;
-            } else {
-                float vb = bl;
-                vb = vb + -0.362267051518f * by[o];
-                vb = vb * 49.87984651440f;
-                P.lf[2][i] = vb;
+        __syncthreads();
+        if (!ok[c]) return;  // uniform: every thread reads the same flag
+        lf_col_plane<kTile>(P, box[b], invy, c, X0, Y0, by);
+        if (c == 0) {
+            __syncthreads();  // every thread has read box 0
+            if (tid == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                lf_box_load(&maps.m[2], box[0], &bar[0], X0, Y0 - kLfR);
             }
         }
     }
@@ -844,6 +932,43 @@ __global__ void copy_window_kernel(const float* src, int64_t src_pitch, int64_t 
 // Engine
 // ------------------------------------------------------------------------------------------
 
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library links only the
+// CUDA runtime); null if the driver does not provide it.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            (void)cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// Tensor map of a dense w x h float plane read in boxes of 32 x kLfVIn, zero outside the
+// plane.  False when a tensor map cannot describe the plane (row pitch not a multiple of 16
+// bytes, base not 16-byte aligned) or the driver refuses it: the caller then uses the
+// plain-load column pass.
+static bool encode_plane_map(CUtensorMap* m, const float* base, int w, int h) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || w % 4 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+    const cuuint64_t dim[2] = {(cuuint64_t)w, (cuuint64_t)h};
+    const cuuint64_t stride[1] = {(cuuint64_t)w * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kTile, (cuuint32_t)kLfVIn};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dim, stride, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 class Engine final : public ButterApi {
 public:
     ~Engine() override { release(); }
@@ -881,10 +1006,34 @@ public:
         partials_ = device_alloc<double>((size_t)nblocks_ * 3, "norm partials");
         norms_d_ = device_alloc<double>(3, "norms");
         norms_host_ = pinned_alloc<double>(3, "norms");
+        // Error word of the tensor-map column pass, in mapped pinned memory so that a call can
+        // read what an earlier asynchronous call reported without synchronising.
+        CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&tma_err_host_), sizeof(int), cudaHostAllocMapped));
+        *tma_err_host_ = 0;
+        CUDA_CHECK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&tma_err_dev_), tma_err_host_, 0));
+        const int w1 = (w_ - 1) / 2 + 1, h1 = (h_ - 1) / 2 + 1;
+        for (int sc = 0; sc < 2; sc++) {
+            const int w = sc ? w1 : w_, h = sc ? h1 : h_;
+            bool ok = true;
+            for (int im = 0; im < 2; im++) {
+                const Planes P = planes_of(im, w, h, sc == 1);
+                for (int c = 0; c < 3; c++) ok = ok && encode_plane_map(&lf_maps_[im][sc].m[c], P.mf[c], w, h);
+            }
+            lf_tma_[sc] = ok;
+        }
+    }
+
+    // Reports (once) a tensor-map load that an earlier call gave up waiting for.
+    void check_tma_error() {
+        if (tma_err_host_ && *(volatile int*)tma_err_host_) {
+            *(volatile int*)tma_err_host_ = 0;
+            VSHIP_THROW(Vship_HIPError, "a tensor-memory load of the low-frequency blur did not complete in time");
+        }
     }
 
     void compute(double norms[3], uint8_t* dstp, int64_t dststride, const uint8_t* const s1[3], const uint8_t* const s2[3],
                  const int64_t ls1[3], const int64_t ls2[3]) override {
+        check_tma_error();
         CUDA_CHECK(cudaStreamWaitEvent(stream_, last_done_, 0));
         RawImage raw[2];
         ColourParams cp[2] = {cp_[0], cp_[1]};
@@ -906,10 +1055,12 @@ public:
         CUDA_CHECK(cudaEventRecord(last_done_, stream_));
         CUDA_CHECK(cudaStreamSynchronize(stream_));
         for (int k = 0; k < 3; k++) norms[k] = norms_host_[k];
+        check_tma_error();
     }
 
     void compute_device(double* d_norms, float* d_distmap, int64_t dststride, const uint8_t* const d1[3],
                         const uint8_t* const d2[3], const int64_t ls1[3], const int64_t ls2[3], cudaStream_t stream) override {
+        check_tma_error();
         ColourParams cp[2] = {cp_[0], cp_[1]};
         RawImage raw[2];
         for (int c = 0; c < 2; c++) {
@@ -986,7 +1137,11 @@ private:
             t = timer_.begin(1, "butter_lf", si);
             lf_row_kernel<<<dim3((unsigned)ceil_div(w, kLfHW), (unsigned)ceil_div(h, 32), 3u), 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
-            lf_col_kernel<<<dim3((unsigned)ceil_div(w, kTile), (unsigned)ceil_div(h, kLfVRows)), 256, 0, si>>>(P[im]);
+            const dim3 cgrid((unsigned)ceil_div(w, kTile), (unsigned)ceil_div(h, kLfVRows));
+            if (lf_tma_[half ? 1 : 0])
+                lf_col_tma_kernel<<<cgrid, 256, 0, si>>>(P[im], lf_maps_[im][half ? 1 : 0], tma_err_dev_);
+            else
+                lf_col_kernel<<<cgrid, 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
             timer_.end(t, si);
             t = timer_.begin(2, "butter_mf", si);
@@ -1073,6 +1228,8 @@ private:
         device_free(norms_d_);
         device_free(distmap_d_);
         pinned_free(norms_host_);
+        if (tma_err_host_) (void)cudaFreeHost(tma_err_host_);
+        tma_err_host_ = tma_err_dev_ = nullptr;
         pool_ = nullptr; partials_ = nullptr; norms_d_ = nullptr; distmap_d_ = nullptr; norms_host_ = nullptr;
         if (last_done_) {
             (void)cudaEventDestroy(last_done_);
@@ -1111,6 +1268,10 @@ private:
     float* distmap_d_ = nullptr;
     cudaEvent_t last_done_ = nullptr;  // completion of the previous call, on whichever stream it ran
     cudaStream_t aux_ = nullptr;       // second stream: the distorted image's per-image kernels
+    LfColMaps lf_maps_[2][2] = {};     // [image][scale]: tensor maps of the mf planes
+    bool lf_tma_[2] = {false, false};  // [scale]: the tensor-map column pass applies
+    int* tma_err_host_ = nullptr;      // mapped pinned error word of that pass
+    int* tma_err_dev_ = nullptr;
     cudaEvent_t fork_ = nullptr, join_ = nullptr;
     KernelTimer timer_;
 };
