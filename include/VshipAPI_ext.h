@@ -52,6 +52,14 @@ EXPORTPREPROCESS Vship_Exception VshipExt_SSIMU2KernelTiming(Vship_SSIMU2Handler
  * reset) and returns their number; reset != 0 clears the totals afterwards.  Synchronises. */
 EXPORTPREPROCESS int VshipExt_SSIMU2KernelTimes(Vship_SSIMU2Handler handler, VshipExt_KernelTime* out, int max, int reset);
 EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliKernelTiming(Vship_ButteraugliHandler handler, int enable);
+/* Test hook for the bounded waits of the low-frequency blur's column pass, which loads its
+ * boxes with tensor-map copies when the plane width is a multiple of 4: in the next call one
+ * box barrier of the reference image's full-scale pass is armed with no copy behind it, so its
+ * wait gives up after a short limit and sets the handler's error word; Vship_ComputeButteraugli
+ * then fails with Vship_HIPError (VshipExt_ComputeButteraugliDevice reports it on the next
+ * call), and the calls after it are whole again.  Nothing faults and the context stays
+ * usable.  Vship_BadDeviceArgument when the handler's resolution does not use that pass. */
+EXPORTPREPROCESS Vship_Exception VshipExt_ButteraugliTestTmaTimeout(Vship_ButteraugliHandler handler);
 EXPORTPREPROCESS int VshipExt_ButteraugliKernelTimes(Vship_ButteraugliHandler handler, VshipExt_KernelTime* out, int max, int reset);
 
 /* Scores one frame pair already in device memory without allocating anything, for callers

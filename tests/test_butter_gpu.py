@@ -92,3 +92,39 @@ def test_concurrent_handlers_on_own_streams(gpu):
     finally:
         for x in hs:
             x.close()
+
+
+def test_tma_wait_limit_reports_error_and_recovers(gpu):
+    """The column pass's bounded tensor-map waits (widths a multiple of 4 take that pass): the
+    test hook arms one box barrier with no copy behind it, the wait gives up, and the call fails
+    with Vship_HIPError instead of hanging; the next call is whole again, through both APIs."""
+    import torch
+    w, h = 256, 128
+    p1, p2, ls = synth.make_pairs(1, w, h, fmt="rgb8", seed=33, blur=(0.0, 1.5))[0]
+    cs = abi.srgb8(w, h)
+    with api.Butteraugli(cs, qnorm=5, intensity=203.0) as hb:
+        good, gmap = hb.compute(p1, p2, ls, distmap=True)
+        hb.test_tma_timeout()
+        with pytest.raises(api.VshipError) as e:
+            hb.compute(p1, p2, ls)
+        assert e.value.code == abi.HIPError
+        again, amap = hb.compute(p1, p2, ls, distmap=True)
+        assert again == good
+        np.testing.assert_array_equal(amap, gmap)
+        # device API: the failure is reported by the call after the one that met it
+        d1 = [torch.from_numpy(p.copy()).cuda() for p in p1]
+        d2 = [torch.from_numpy(p.copy()).cuda() for p in p2]
+        norms = torch.zeros(3, dtype=torch.float64, device="cuda")
+        hb.test_tma_timeout()
+        hb.compute_device([t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls, ls, norms.data_ptr())
+        torch.cuda.synchronize()
+        with pytest.raises(api.VshipError):
+            hb.compute_device([t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls, ls, norms.data_ptr())
+        hb.compute_device([t.data_ptr() for t in d1], [t.data_ptr() for t in d2], ls, ls, norms.data_ptr())
+        torch.cuda.synchronize()
+        assert tuple(norms.cpu().numpy()) == tuple(good)
+    odd = abi.srgb8(258, 128)
+    with api.Butteraugli(odd, qnorm=5, intensity=203.0) as hb:
+        with pytest.raises(api.VshipError) as e:
+            hb.test_tma_timeout()
+        assert e.value.code == abi.BadDeviceArgument

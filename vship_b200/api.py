@@ -85,6 +85,7 @@ def _declare(L):
     L.VshipExt_ComputeSSIMU2NoAlloc.argtypes = [abi.Colorspace, abi.Colorspace, c.c_void_p, c.c_void_p, vpp, vpp,
                                                 i64p, i64p, c.c_void_p]
     L.VshipExt_ButteraugliResolution.argtypes = [HB, i64p, i64p]
+    L.VshipExt_ButteraugliTestTmaTimeout.argtypes = [HB]
     HBt = abi.SSIMU2BatchHandler
     FPp = c.POINTER(abi.FramePair)
     L.VshipExt_SSIMU2BatchInit.argtypes = [c.POINTER(HBt), c.c_int]
@@ -315,6 +316,10 @@ class Butteraugli:
 
     def kernel_timing(self, enable=True):
         check(self.L, self.L.VshipExt_ButteraugliKernelTiming(self.h, 1 if enable else 0))
+
+    def test_tma_timeout(self):
+        """Arms the next call's test of the column pass's bounded tensor-map waits."""
+        check(self.L, self.L.VshipExt_ButteraugliTestTmaTimeout(self.h), self.L.Vship_ButteraugliGetDetailedLastError, self.h)
 
     def kernel_times(self, reset=False):
         out = (KernelTime * 8)()

@@ -676,6 +676,15 @@ int VshipExt_ButteraugliKernelTimes(Vship_ButteraugliHandler handler, VshipExt_K
     return kernel_times(g_butter, handler.id, out, max, reset);
 }
 
+Vship_Exception VshipExt_ButteraugliTestTmaTimeout(Vship_ButteraugliHandler handler) {
+    return with_handler(g_butter, handler.id, "VshipExt_ButteraugliTestTmaTimeout", [&](Slot<ButterApi>& s) {
+        require_engine((bool)s.engine);
+        if (!s.engine->test_tma_timeout())
+            throw Error(Vship_BadDeviceArgument, __FILE__, __LINE__,
+                        "this handler's resolution does not use the tensor-map column pass");
+    });
+}
+
 Vship_Exception VshipExt_SSIMU2Resolution(Vship_SSIMU2Handler handler, int64_t* width, int64_t* height) {
     return with_handler(g_ssimu2, handler.id, "VshipExt_SSIMU2Resolution", [&](Slot<Ssimu2Api>& s) {
         require_engine((bool)s.engine);

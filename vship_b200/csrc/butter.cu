@@ -503,6 +503,7 @@ struct LfColMaps {
 
 constexpr unsigned kLfBoxBytes = kLfVIn * kTile * sizeof(float);
 constexpr long long kTmaWaitLimit = 1ll << 24;  // polls of a box's barrier before giving up
+constexpr long long kTmaTestWaitLimit = 1ll << 12;  // the same under the test hook
 
 __device__ __forceinline__ void lf_box_load(const CUtensorMap* map, float* dst, uint64_t* bar, int x, int y) {
     const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
@@ -513,10 +514,10 @@ __device__ __forceinline__ void lf_box_load(const CUtensorMap* map, float* dst, 
         : "memory");
 }
 
-// Polls the barrier's phase `parity` at most kTmaWaitLimit times; false if it did not complete.
-__device__ __forceinline__ bool lf_box_wait(uint64_t* bar, unsigned parity) {
+// Polls the barrier's phase `parity` at most `limit` times; false if it did not complete.
+__device__ __forceinline__ bool lf_box_wait(uint64_t* bar, unsigned parity, long long limit) {
     const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
-    for (long long i = 0; i < kTmaWaitLimit; i++) {
+    for (long long i = 0; i < limit; i++) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -526,8 +527,10 @@ __device__ __forceinline__ bool lf_box_wait(uint64_t* bar, unsigned parity) {
     return false;
 }
 
+// `test_skip`: the test hook's launch; plane 0's barrier is armed but its box is never
+// loaded, so its wait runs out (after kTmaTestWaitLimit polls) and the error path runs.
 __global__ void __launch_bounds__(256, 5) lf_col_tma_kernel(Planes P, const __grid_constant__ LfColMaps maps,
-                                                            int* __restrict__ err) {
+                                                            int* __restrict__ err, int test_skip) {
     __shared__ alignas(128) float box[2][kLfVIn * kTile];
     __shared__ float invy[kLfVRows];
     __shared__ alignas(8) uint64_t bar[2];
@@ -538,9 +541,14 @@ __global__ void __launch_bounds__(256, 5) lf_col_tma_kernel(Planes P, const __gr
         for (int b = 0; b < 2; b++)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&bar[b])) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        lf_box_load(&maps.m[0], box[0], &bar[0], X0, Y0 - kLfR);
+        if (test_skip)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                         ::"r"((uint32_t)__cvta_generic_to_shared(&bar[0])), "r"(kLfBoxBytes) : "memory");
+        else
+            lf_box_load(&maps.m[0], box[0], &bar[0], X0, Y0 - kLfR);
         lf_box_load(&maps.m[1], box[1], &bar[1], X0, Y0 - kLfR);
     }
+    const long long limit = test_skip ? kTmaTestWaitLimit : kTmaWaitLimit;
     if (tid < kLfVRows) invy[tid] = 1.0f / tap_sum(kLfK, kLfR, min(Y0 + tid, h - 1), h);
     float by[kLfRPT];
 #pragma unroll 1
@@ -548,8 +556,14 @@ __global__ void __launch_bounds__(256, 5) lf_col_tma_kernel(Planes P, const __gr
         const int b = c & 1;
         // One thread waits for the box; the barrier then hands its data to the whole CTA.
         if (tid == 0) {
-            ok[c] = lf_box_wait(&bar[b], (unsigned)(c >> 1));
-            if (!ok[c]) atomicExch(err, 1);
+            ok[c] = lf_box_wait(&bar[b], (unsigned)(c >> 1), limit);
+            if (!ok[c]) {
+                *(volatile int*)err = 1;  // mapped host memory: a plain store (every writer stores 1)
+                // Before the CTA leaves, the other box still loading must land: plane 1's
+                // (issued at the start) while plane 0 is awaited, plane 2's while plane 1 is.
+                if (c == 0) (void)lf_box_wait(&bar[1], 0u, kTmaWaitLimit);
+                if (c == 1) (void)lf_box_wait(&bar[0], 1u, kTmaWaitLimit);
+            }
         }
         __syncthreads();
         if (!ok[c]) return;  // uniform: every thread reads the same flag
@@ -1081,6 +1095,12 @@ public:
         CUDA_CHECK(cudaEventRecord(last_done_, stream));
     }
 
+    bool test_tma_timeout() override {
+        if (!lf_tma_[0]) return false;
+        tma_test_ = true;
+        return true;
+    }
+
     KernelTimer& timer() override { return timer_; }
     int width() const override { return w_; }
     int height() const override { return h_; }
@@ -1139,7 +1159,8 @@ private:
             CUDA_CHECK(cudaGetLastError());
             const dim3 cgrid((unsigned)ceil_div(w, kTile), (unsigned)ceil_div(h, kLfVRows));
             if (lf_tma_[half ? 1 : 0])
-                lf_col_tma_kernel<<<cgrid, 256, 0, si>>>(P[im], lf_maps_[im][half ? 1 : 0], tma_err_dev_);
+                lf_col_tma_kernel<<<cgrid, 256, 0, si>>>(P[im], lf_maps_[im][half ? 1 : 0], tma_err_dev_,
+                                                         tma_test_ && im == 0 && !half);
             else
                 lf_col_kernel<<<cgrid, 256, 0, si>>>(P[im]);
             CUDA_CHECK(cudaGetLastError());
@@ -1208,6 +1229,7 @@ private:
         // The half scale reuses the full scale's band planes, which the full-scale diff map reads.
         after(aux, st, fork_);
         scale_pass(w1, h1, true, diffmap(1), st, aux);
+        tma_test_ = false;  // the test hook covers one call
         const int t = timer_.begin(6, "butter_norms", st);
         combine_norms_kernel<<<nblocks_, 256, 0, st>>>(diffmap(0), diffmap(1), w_, h_, w1, qnorm_, distmap, dst_pitch, partials_);
         CUDA_CHECK(cudaGetLastError());
@@ -1272,6 +1294,7 @@ private:
     bool lf_tma_[2] = {false, false};  // [scale]: the tensor-map column pass applies
     int* tma_err_host_ = nullptr;      // mapped pinned error word of that pass
     int* tma_err_dev_ = nullptr;
+    bool tma_test_ = false;            // the test hook's next call
     cudaEvent_t fork_ = nullptr, join_ = nullptr;
     KernelTimer timer_;
 };

@@ -40,6 +40,10 @@ struct ButterApi {
     virtual void compute_device(double* d_norms, float* d_distmap, int64_t dststride, const uint8_t* const d1[3],
                                 const uint8_t* const d2[3], const int64_t ls1[3], const int64_t ls2[3],
                                 cudaStream_t stream) = 0;
+    // Test hook: the next call's full-scale low-frequency column pass of the reference image
+    // leaves one box barrier armed with no load behind it, so that wait runs out.  False when
+    // this handler's resolution does not use the tensor-map pass.
+    virtual bool test_tma_timeout() = 0;
     virtual KernelTimer& timer() = 0;
     virtual int width() const = 0;
     virtual int height() const = 0;
