@@ -229,8 +229,50 @@ static __global__ void __launch_bounds__(256) ingest_linear_kernel(RawImage im, 
     }
 }
 
+// Linear RGB of 8-bit R'G'B' sRGB planes (the kFastRgb8Srgb colourspaces): four pixels of a
+// row per thread, one 32-bit load per plane when the four samples are 4-byte aligned and one
+// float4 store per plane when the output is; each value is ingest_fast<kFastRgb8Srgb>'s.
+static __global__ void __launch_bounds__(256) ingest_linear_rgb8_kernel(RawImage im, ColourParams cp, float* out,
+                                                                       int64_t plane_stride) {
+    const int64_t qw = (cp.W + 3) / 4;
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t Y = q / qw, X = (q - Y * qw) * 4;
+    if (Y >= cp.H) return;
+    const int n = (int)min((int64_t)4, cp.W - X);
+    const int64_t o = Y * cp.W + X;
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        const uint8_t* src = im.p[p] + Y * im.stride[p] + X;
+        float v[4];
+        if (n == 4 && (reinterpret_cast<uintptr_t>(src) & 3) == 0) {
+            const uchar4 u = __ldg(reinterpret_cast<const uchar4*>(src));
+            v[0] = srgb_to_linear(range_luma((float)u.x, cp));
+            v[1] = srgb_to_linear(range_luma((float)u.y, cp));
+            v[2] = srgb_to_linear(range_luma((float)u.z, cp));
+            v[3] = srgb_to_linear(range_luma((float)u.w, cp));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[k] = k < n ? srgb_to_linear(range_luma((float)__ldg(src + k), cp)) : 0.f;
+        }
+        float* dst = out + p * plane_stride + o;
+        if (n == 4 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (k < n) dst[k] = v[k];
+        }
+    }
+}
+
 inline void launch_ingest_linear(const RawImage& im, const ColourParams& cp, float* out, int64_t plane_stride, cudaStream_t st,
                                  bool native = false) {
+    if (!native && fast_path_of(cp) == kFastRgb8Srgb) {
+        const int64_t quads = (cp.W + 3) / 4 * cp.H;
+        ingest_linear_rgb8_kernel<<<(unsigned)ceil_div(quads, 256), 256, 0, st>>>(im, cp, out, plane_stride);
+        CUDA_CHECK(cudaGetLastError());
+        return;
+    }
     const dim3 grid((unsigned)ceil_div(cp.W, kStageTile), (unsigned)ceil_div(cp.H, kStageTile));
     const size_t smem = sizeof(float) * chroma_stage_floats(cp.subw, cp.subh);
     auto kernel = native ? ingest_linear_kernel<true> : ingest_linear_kernel<false>;
