@@ -342,27 +342,31 @@ constexpr int kLfR = 21;
 constexpr int kLfNT = 2 * kLfR + 1;
 constexpr int kLfK = 4;                 // tap set of sigma 7.16
 constexpr int kLfHW = 128;              // row pass: 32 rows x 128 columns per CTA
-constexpr int kLfHIn = kLfHW + 2 * kLfR;
 constexpr int kLfVRows = 64;            // column pass: 64 rows x 32 columns per CTA
 constexpr int kLfRPT = kLfVRows / 8;    // rows per thread
 constexpr int kLfVIn = kLfVRows + 2 * kLfR;
 
-struct LfRowSmem {
-    float in[32][kLfHIn + 1];   // odd pitch: lanes on consecutive rows read without conflicts
-    float out[32][kLfHW + 1];
-    float invx[kLfHW];
-};
+// Row pass of plane blockIdx.z: xyb -> mf (horizontal blur, renormalised per column).  The
+// CTA stages a dense box of 32 rows x kLfHBox columns starting kLfHPad columns left of its
+// first output (the halo rounded out to a multiple of 4, so that every 4-column group of the
+// box is a 16-byte word); warp k blurs rows k, k + 8, k + 16, k + 24 and lane l the outputs
+// 4l .. 4l + 3 of a row, reading its 52-column window as 13 float4 (a warp reads 512
+// consecutive bytes: no bank conflicts) and writing its four outputs as one float4 when the
+// plane row allows.  Per output, the taps are applied in the same order as in blur_tile.
+constexpr int kLfHPad = (kLfR + 3) / 4 * 4;        // 24
+constexpr int kLfHBox = kLfHW + 2 * kLfHPad;       // 176
+constexpr int kLfHWin = (3 + kLfNT + 3 + 3) / 4;   // float4 per lane window: 13
 
-// Row pass of plane blockIdx.z: xyb -> mf (horizontal blur, renormalised per column).
 __global__ void __launch_bounds__(256) lf_row_kernel(Planes P) {
-    __shared__ LfRowSmem sm;
+    __shared__ alignas(16) float in[32][kLfHBox];
+    __shared__ float invx[kLfHW];
     const int c = blockIdx.z;
     const int X0 = blockIdx.x * kLfHW, Y0 = blockIdx.y * 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int w = P.w, h = P.h;
     const float* src = P.xyb[c];
     // Staging: warp k takes rows k, k + 8, k + 16, k + 24; lanes the columns.
-    constexpr int kCols = (kLfHIn + 31) / 32;
+    constexpr int kCols = (kLfHBox + 31) / 32;
 #pragma unroll
     for (int s = 0; s < 4; s++) {
         const int r = warp + 8 * s, gy = Y0 + r;
@@ -371,22 +375,32 @@ __global__ void __launch_bounds__(256) lf_row_kernel(Planes P) {
         float v[kCols];
 #pragma unroll
         for (int k = 0; k < kCols; k++) {
-            const int cc = lane + 32 * k, gx = X0 - kLfR + cc;
-            v[k] = (rowin && cc < kLfHIn && (unsigned)gx < (unsigned)w) ? row[gx] : 0.f;
+            const int cc = lane + 32 * k, gx = X0 - kLfHPad + cc;
+            v[k] = (rowin && cc < kLfHBox && (unsigned)gx < (unsigned)w) ? row[gx] : 0.f;
         }
 #pragma unroll
         for (int k = 0; k < kCols; k++)
-            if (lane + 32 * k < kLfHIn) sm.in[r][lane + 32 * k] = v[k];
+            if (lane + 32 * k < kLfHBox) in[r][lane + 32 * k] = v[k];
     }
-    if (tid < kLfHW) sm.invx[tid] = 1.0f / tap_sum(kLfK, kLfR, min(X0 + tid, w - 1), w);
+    if (tid < kLfHW) invx[tid] = 1.0f / tap_sum(kLfK, kLfR, min(X0 + tid, w - 1), w);
     __syncthreads();
-    // A work item is four adjacent outputs of one row; consecutive threads take consecutive rows.
-    for (int u = tid; u < 32 * (kLfHW / 4); u += 256) {
-        const int r = u & 31, c0 = (u >> 5) * 4;
+    float* dst = P.mf[c];
+    const int c0 = 4 * lane;  // first output of the lane; its taps start at box column c0 + 3
+    const int gx0 = X0 + c0;
+#pragma unroll 1
+    for (int s = 0; s < 4; s++) {
+        const int r = warp + 8 * s, gy = Y0 + r;
+        if (gy >= h) break;  // uniform over the warp
+        float win[4 * kLfHWin];
+#pragma unroll
+        for (int m = 0; m < kLfHWin; m++) {
+            const float4 q = *reinterpret_cast<const float4*>(&in[r][c0 + 4 * m]);
+            win[4 * m] = q.x; win[4 * m + 1] = q.y; win[4 * m + 2] = q.z; win[4 * m + 3] = q.w;
+        }
         float a[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int j = 0; j < kLfNT + 3; j++) {
-            const float v = sm.in[r][c0 + j];
+            const float v = win[kLfHPad - kLfR + j];
 #pragma unroll
             for (int o = 0; o < 4; o++) {
                 const int t = j - o;
@@ -394,18 +408,15 @@ __global__ void __launch_bounds__(256) lf_row_kernel(Planes P) {
             }
         }
 #pragma unroll
-        for (int o = 0; o < 4; o++) sm.out[r][c0 + o] = a[o] * sm.invx[c0 + o];
-    }
-    __syncthreads();
-    float* dst = P.mf[c];
+        for (int o = 0; o < 4; o++) a[o] = a[o] * invx[c0 + o];
+        if (gx0 >= w) continue;
+        float* out = dst + (int64_t)gy * w + gx0;
+        if (gx0 + 4 <= w && (reinterpret_cast<uintptr_t>(out) & 15) == 0) {
+            *reinterpret_cast<float4*>(out) = make_float4(a[0], a[1], a[2], a[3]);
+        } else {
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-        const int r = warp + 8 * s, gy = Y0 + r;
-        if (gy >= h) break;
-#pragma unroll
-        for (int k = 0; k < kLfHW / 32; k++) {
-            const int gx = X0 + lane + 32 * k;
-            if (gx < w) dst[(int64_t)gy * w + gx] = sm.out[r][lane + 32 * k];
+            for (int o = 0; o < 4; o++)
+                if (gx0 + o < w) out[o] = a[o];
         }
     }
 }
